@@ -1,0 +1,198 @@
+/*
+ * pcc_gpu.h -- C ABI of the B200 (sm_100a) collision hot path of the
+ * ProliferatingCellCollectives simulator.
+ *
+ * One context (pcc_ctx) holds one colony resident on one GPU.  Every entry
+ * point returns a pcc_status (0 = PCC_OK); pcc_last_error() gives the message
+ * of the last failure on a context.  Calls on one context are not
+ * thread-safe: use one host thread per context.  All state arrays that cross
+ * this boundary are caller-owned host buffers in structure-of-arrays form;
+ * they are copied, never retained.
+ *
+ * Reference interfaces replaced (paths are inside the reference project,
+ * under code/cpp/src/):
+ *   pcc_solve            ParticleManager::step (simulation/ParticleManager.cpp:150-166)
+ *                        -> solveHardModel (dynamics/models/Hard.h:9, Hard.cpp:91-192)
+ *                        -> solveSoftPotential (dynamics/models/Soft.h:8, Soft.cpp:21-114)
+ *   pcc_step             one iteration of Domain::run at one rank
+ *                        (spatial/Domain.cpp:120-153): divideParticles + commit,
+ *                        assignGlobalIDs (492-508), step, adaptDt (69-118), radius
+ *   pcc_detect_contacts  CollisionDetector::detectCollisions (spatial/CollisionDetector.cpp:84-111)
+ *   pcc_get_constraints  SolverSolution::constraints (simulation/ParticleManager.h:33-39)
+ *   pcc_bbpgd_frozen     BBPGD (solver/BBPGD.h:26-31) on a frozen constraint set
+ *   pcc_soft_forces_frozen  the Hertz force loop of solveSoftPotential (Soft.cpp:46-83)
+ * Errors that the reference raises as std::runtime_error come back as
+ * PCC_ERR_NOCONV_BBPGD ("BBPGD did not converge", solver/BBPGD.cpp:118-121) and
+ * PCC_ERR_NOCONV_RELCP ("Maximum number of constraint iterations reached",
+ * dynamics/models/Hard.cpp:187-190).
+ */
+#ifndef PCC_GPU_H
+#define PCC_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int pcc_status;
+#define PCC_OK 0
+#define PCC_ERR_INVALID 1       /* bad argument or call order */
+#define PCC_ERR_NOCONV_BBPGD 2  /* BBPGD hit max_bbpgd_iterations */
+#define PCC_ERR_NOCONV_RELCP 3  /* ReLCP hit max_recursive_iterations */
+#define PCC_ERR_CAPACITY 4      /* caller buffer too small; *n holds the size needed */
+#define PCC_ERR_TIMEOUT 5       /* a bounded device-side wait gave up */
+#define PCC_ERR_BOUNDS 6        /* a device-side bounds check failed */
+#define PCC_ERR_CUDA 7          /* CUDA runtime error */
+#define PCC_ERR_NAN 8           /* non-finite state detected */
+#define PCC_ERR_NOMEM 9         /* device allocation failed */
+
+#define PCC_MODE_HARD 0
+#define PCC_MODE_SOFT 1
+
+/* What the per-phase ghost exchange of the reference driver supplies at one
+ * rank (Domain::exchangeGhostParticles, spatial/Domain.cpp:339-403): at world
+ * size 1 the angular-neighbour test picks the rank itself, so every cell with
+ * |(x,y)| >= 8 whose distance to the 0/360-degree sector edge is below 2.5
+ * becomes a ghost copy of itself.  The ownership rule of
+ * CollisionDetector::tryCreateConstraint (spatial/CollisionDetector.cpp:261-275)
+ * then emits a second, identical constraint for every contact whose
+ * larger-id cell has such a copy.  PCC_GHOSTS_SINGLE_RANK reproduces that;
+ * PCC_GHOSTS_NONE is the same solver with no ghost copies. */
+#define PCC_GHOSTS_NONE 0
+#define PCC_GHOSTS_SINGLE_RANK 1
+
+#define PCC_PRECISION_FP64 0
+
+/* Mirrors SimulationParameters (util/Config.h:27-56, defaults in
+ * util/CLIParser.h:296-365) plus the run-time switches of this library. */
+typedef struct pcc_params {
+  /* SimulationConfig */
+  double dt;          /* -dt: first (or fixed) time step */
+  double end_radius;  /* -end_radius: pcc_run stops once the colony radius reaches it */
+  /* PhysicsConfig */
+  double xi;          /* -xi: drag per unit length */
+  double tau;         /* -tau: growth time constant */
+  double l0;          /* -l0: birth length; cells divide at 2*l0 */
+  double lambda;      /* -lambda: stress sensitivity of growth */
+  double temperature; /* -temperature: must be 0 here (Brownian kicks are not on the device path) */
+  double kcc;         /* -kcc: Hertz constant of the soft model */
+  int monolayer;      /* -monolayer (only affects Brownian kicks) */
+  /* SolverConfig */
+  double tolerance;                    /* -tolerance: BBPGD residual, ReLCP overlap, CFL */
+  long long max_bbpgd_iterations;      /* -max_bbpgd_iterations */
+  long long max_recursive_iterations;  /* -max_recursive_iterations */
+  double linked_cell_size;             /* -linked_cell_size (2.2*l0 when unset) */
+  double cfl_factor;                   /* -cfl_factor */
+  /* -mode */
+  int mode;                            /* PCC_MODE_HARD or PCC_MODE_SOFT */
+  /* additions (default off) */
+  int fixed_dt;                        /* 1: skip adaptDt, keep dt */
+  double dt_cap;                       /* > 0: adapted dt never exceeds this */
+  int ghost_mode;                      /* PCC_GHOSTS_* */
+  unsigned long long seed;             /* seeds the division length draws */
+  int precision;                       /* PCC_PRECISION_FP64 */
+  long long capacity_hint;             /* expected peak cell count (0: grow on demand) */
+} pcc_params;
+
+/* Host SoA view of n cells (index = global id after the x-sort).  Optional
+ * arrays may be NULL.  force/velocity hold 6 values per cell (linear, angular). */
+typedef struct pcc_cells {
+  double *x, *y, *z;           /* centre */
+  double *q0, *q1, *q2, *q3;   /* unit quaternion (w, x, y, z) */
+  double *length, *l0, *diameter;
+  double *ldot, *impedance, *stress;  /* optional */
+  int *age;                           /* optional */
+  double *force, *velocity;           /* optional, 6 per cell */
+} pcc_cells;
+
+/* Host SoA view of constraints (Constraint, dynamics/Constraint.h:6-49). */
+typedef struct pcc_contacts {
+  int *gid_i, *gid_j;
+  double *sd;            /* signed distance (phi) */
+  double *normal;        /* 3 per contact: normI, unit, from j towards i */
+  double *r_i, *r_j;     /* 3 each: contact point minus centre */
+  double *contact_point; /* 3 */
+  double *stress_i, *stress_j;
+  double *gamma;
+  int *phase;            /* ReLCP iteration that detected it */
+} pcc_contacts;
+
+/* SolverSolution scalars (simulation/ParticleManager.h:33-39) plus driver data. */
+typedef struct pcc_step_stats {
+  int relcp_iterations;         /* constraint_iterations */
+  long long bbpgd_iterations;   /* summed over ReLCP phases */
+  double residual;
+  double max_overlap;
+  long long n_constraints;      /* size of the returned constraint set */
+  long long n_cells;            /* cells during the solve */
+  long long n_divided;          /* divisions committed at the start of the step */
+  double dt_used;               /* dt of this step */
+  double dt_next;               /* dt after adaptDt */
+  double colony_radius;         /* after the step */
+  double sim_time;              /* after the step */
+} pcc_step_stats;
+
+typedef struct pcc_ctx pcc_ctx;
+
+/* Reference defaults (CLIParser.h:296-365), mode hard, ghosts NONE. */
+void pcc_default_params(pcc_params* p);
+
+pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out);
+pcc_status pcc_destroy(pcc_ctx* ctx);
+const char* pcc_last_error(const pcc_ctx* ctx);
+
+/* Runtime parameters that the driver may change between steps. */
+pcc_status pcc_set_dt(pcc_ctx* ctx, double dt);
+pcc_status pcc_get_dt(const pcc_ctx* ctx, double* dt);
+
+/* Replace the colony with n cells (copied).  Any order; pcc_step sorts. */
+pcc_status pcc_upload_cells(pcc_ctx* ctx, const pcc_cells* cells, size_t n);
+/* Copy the colony out in global-id order.  PCC_ERR_CAPACITY if cap < n. */
+pcc_status pcc_download_cells(pcc_ctx* ctx, pcc_cells* cells, size_t cap, size_t* n);
+pcc_status pcc_cell_count(const pcc_ctx* ctx, size_t* n);
+
+/* One solver call on the resident cells, which must already be in global-id
+ * order (ParticleManager::step): ReLCP/BBPGD (hard) or Hertz forces (soft),
+ * then move, set growth parameters and grow with time step dt. */
+pcc_status pcc_solve(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* out);
+
+/* One Domain::run iteration: divide, append daughters, sort by x and
+ * renumber, pcc_solve, advance time, adapt dt (unless fixed), colony radius. */
+pcc_status pcc_step(pcc_ctx* ctx, pcc_step_stats* out);
+
+/* Repeat pcc_step until the colony radius reaches end_radius or max_steps
+ * steps ran.  Sums cells over steps into *cell_steps when non-NULL. */
+pcc_status pcc_run(pcc_ctx* ctx, double end_radius, long long max_steps, long long* steps_done,
+                   double* cell_steps, pcc_step_stats* last);
+
+/* Contact detection on the resident state with tolerance tol (phase is
+ * recorded in the output).  Order: grouped by the smaller global id. */
+pcc_status pcc_detect_contacts(pcc_ctx* ctx, double tol, int phase, pcc_contacts* out, size_t cap, size_t* n);
+
+/* The constraint set returned by the last pcc_solve (after write-back). */
+pcc_status pcc_get_constraints(pcc_ctx* ctx, pcc_contacts* out, size_t cap, size_t* n);
+
+/* Microbench / parity entry points on a frozen state. */
+pcc_status pcc_bbpgd_frozen(pcc_ctx* ctx, double dt, int repeats, long long* iterations, double* residual,
+                            float* ms_per_solve);
+pcc_status pcc_soft_forces_frozen(pcc_ctx* ctx, int repeats, float* ms_per_assembly);
+
+/* The CUDA stream all work of the context is queued on (a cudaStream_t). */
+void* pcc_get_stream(const pcc_ctx* ctx);
+
+/* Kernel launches issued by this context so far (for launch accounting). */
+long long pcc_launch_count(const pcc_ctx* ctx);
+
+/* Division length draw used by the device (exposed for tests): the length of
+ * the left daughter of a cell of length len, for the k-th division of a
+ * colony seeded with seed -- std::mt19937 seeded with pcc_division_seed(seed, k),
+ * then std::uniform_real_distribution<double>(0.98*len/2, 1.02*len/2). */
+unsigned int pcc_division_seed(unsigned long long seed, unsigned long long k);
+double pcc_division_length_host(unsigned long long seed, unsigned long long k, double len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PCC_GPU_H */

@@ -1,0 +1,3 @@
+// Single-rank PETSc stand-in for the oracle build: everything lives in petsc.h.
+#pragma once
+#include <petsc.h>
