@@ -135,7 +135,8 @@ typedef struct pcc_step_stats {
 
 typedef struct pcc_ctx pcc_ctx;
 
-/* Reference defaults (CLIParser.h:296-365), mode hard, ghosts NONE. */
+/* Reference defaults (CLIParser.h:296-365): hard mode, temperature 0, ghost
+ * copies as the reference driver makes them at one rank (PCC_GHOSTS_SINGLE_RANK). */
 void pcc_default_params(pcc_params* p);
 
 pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out);

@@ -1,0 +1,133 @@
+// Host-side context of one resident colony: device buffers, stream and the
+// per-step orchestration state.  Internal to libpcc_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pcc_common.cuh"
+#include "pcc_gpu.h"
+
+namespace pcc {
+
+// Growable device buffer.  grow() keeps the first `keep` elements.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t reserve(size_t n, size_t keep, cudaStream_t s) {
+    if (n <= cap) return cudaSuccess;
+    size_t nc = cap ? cap : 64;
+    while (nc < n) nc = nc + nc / 2 + 64;
+    T* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, nc * sizeof(T));
+    if (e != cudaSuccess) return e;
+    if (p && keep) {
+      e = cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return e;
+      e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return e;
+    }
+    if (p) cudaFree(p);
+    p = q;
+    cap = nc;
+    return cudaSuccess;
+  }
+};
+
+// All per-cell arrays (one set; the x-sort gathers into a second set and swaps).
+struct CellBufs {
+  DevBuf<double> x, y, z, q0, q1, q2, q3, len, l0, diam, ldot, imp, stress, force, vel;
+  DevBuf<int> age;
+  cudaError_t reserve(size_t n, size_t keep, cudaStream_t s);
+  CellsView view();
+  void swap(CellBufs& o);
+};
+
+struct ConsBufs {
+  DevBuf<int> gi, gj, phase;
+  DevBuf<double> sd, gamma, nx, ny, nz, tix, tiy, tiz, tjx, tjy, tjz, rix, riy, riz, rjx, rjy, rjz, cpx, cpy,
+      cpz, si, sj;
+  cudaError_t reserve(size_t n, size_t keep, cudaStream_t s);
+  ConsView view();
+};
+
+// Grid barrier + reduction scratch of the persistent solver kernel.
+struct SolverScalars {
+  unsigned count;       // arrivals at the current barrier
+  unsigned gen;         // barrier generation
+  int converged;        // 1 once the residual test passed
+  int pad;
+  long long iterations; // BBPGD iteration count at exit
+  double alpha;         // current step size
+  double residual;      // last evaluated residual
+  double res0;          // initial residual
+};
+
+struct Timers {
+  double detect_ms = 0, solve_ms = 0, update_ms = 0;
+};
+
+}  // namespace pcc
+
+struct pcc_ctx {
+  pcc_params params{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  int num_sms = 0;
+  std::string err;
+
+  size_t n = 0;  // resident cells
+  pcc::CellBufs cells, cells_alt;
+
+  // constraints accumulated during the current step
+  size_t ncons = 0;
+  pcc::ConsBufs cons;
+
+  // detection scratch
+  pcc::DevBuf<int> bin_of, bin_cnt, bin_off, bin_cursor, bin_cells, cand_cnt, cand_off;
+  pcc::DevBuf<double> pk;  // packed per-cell geometry in bin order
+  pcc::DevBuf<int> ghost;
+  pcc::DevBuf<int> bbox;   // [6] min/max bin coordinates
+
+  // incidence CSR (cell -> constraint sides)
+  pcc::DevBuf<int> inc_cnt, inc_off, inc_ent;
+
+  // solver scratch
+  pcc::DevBuf<double> gam_a, gam_b, g_a, g_b, gam_old;
+  pcc::DevBuf<double> U, dldot, F, sig, ldot_new, imp_new, Mlin, Mrot, ldot_prev;
+  pcc::DevBuf<double> partials;
+  pcc::DevBuf<pcc::SolverScalars> scal;
+  pcc::DevBuf<double> fel;  // soft: Hertz force magnitude per contact
+
+  // step scratch
+  pcc::DevBuf<int> div_flag, div_off;
+  pcc::DevBuf<unsigned long long> keys, keys_alt;
+  pcc::DevBuf<int> perm, perm_alt, sort_hist;
+  pcc::DevBuf<int> scan_tmp;
+  pcc::DevBuf<double> red;  // small reductions
+
+  pcc::DevStatus* status = nullptr;  // device
+  pcc::DevStatus* status_host = nullptr;  // pinned mirror
+  long long* pinned_ll = nullptr;         // pinned scratch for small read-backs
+  double* pinned_d = nullptr;
+
+  unsigned long long div_index = 0;  // divisions so far (RNG stream position)
+  long long iter = 0;
+  double sim_time = 0, radius = 0;
+  long long launches = 0;
+  int coop_blocks = 0;  // co-resident blocks of the solver kernel
+
+  pcc::Timers timers;
+};

@@ -1,0 +1,499 @@
+// Broadphase + narrowphase contact detection (sm_100a).
+//
+// Replaces SpatialGrid::findPotentialCollisions (spatial/SpatialGrid.cpp:58-121)
+// and CollisionDetector::tryCreateConstraint (spatial/CollisionDetector.cpp:201-311)
+// of the reference.  Cells are binned on their centres exactly like the
+// reference grid (origin -1, edge linked_cell_size, floor), so the candidate
+// pairs -- every unordered pair in the same or an adjacent bin of the
+// 27-stencil -- are the same set.  Binning is a counting sort: atomic counts,
+// an exclusive scan, an atomic scatter and a per-bin sort by id, which makes
+// the bin contents (and everything downstream) deterministic.  Each cell's
+// geometry is packed once per phase in bin order so the neighbour scans read
+// contiguous 32-byte groups.  The pair test runs twice (count, then emit into
+// the scanned offsets): constraints come out grouped by the smaller id in a
+// fixed order, without atomics on the output.
+#include <cmath>
+
+#include "pcc_kernels.hpp"
+
+namespace pcc {
+
+namespace {
+
+constexpr int kPack = 16;  // doubles per packed cell record
+// record layout: [x y z len | sx sy sz diam | ex ey ez gid | tx ty tz ghost]
+
+__global__ void k_bin(CellsView c, size_t n, double h, int ghost_mode, int* __restrict__ binxyz,
+                      int* __restrict__ bbox, int* __restrict__ ghost) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = c.x[i], y = c.y[i], z = c.z[i];
+  int bx = (int)floor(dvd(sub(x, -1.0), h));
+  int by = (int)floor(dvd(sub(y, -1.0), h));
+  int bz = (int)floor(dvd(sub(z, -1.0), h));
+  binxyz[3 * i] = bx;
+  binxyz[3 * i + 1] = by;
+  binxyz[3 * i + 2] = bz;
+  atomicMin(&bbox[0], bx);
+  atomicMin(&bbox[1], by);
+  atomicMin(&bbox[2], bz);
+  atomicMax(&bbox[3], bx);
+  atomicMax(&bbox[4], by);
+  atomicMax(&bbox[5], bz);
+  int g = 0;
+  if (ghost_mode == PCC_GHOSTS_SINGLE_RANK) {
+    // Domain::exchangeGhostParticles at world size 1 (spatial/Domain.cpp:339-403)
+    // with calculateDistanceToAngularBoundary (263-290) for the sector [0, 360).
+    double ang = dvd(mul(atan2(y, x), 180.0), M_PI);
+    if (ang < 0) ang += 360.0;
+    double radius = __dsqrt_rn(add(mul(x, x), mul(y, y)));
+    if (radius >= 8.0) {
+      double dmin = ang - 0.0, dmax = 360.0 - ang;
+      while (dmin > 180.0) dmin -= 360.0;
+      while (dmin < -180.0) dmin += 360.0;
+      while (dmax > 180.0) dmax -= 360.0;
+      while (dmax < -180.0) dmax += 360.0;
+      double dist = 0.0;
+      if (!(dmin >= 0 && dmax >= 0)) {
+        double m = fabs(dmin) < fabs(dmax) ? fabs(dmin) : fabs(dmax);
+        dist = mul(radius, sin(dvd(mul(m, M_PI), 180.0)));
+      }
+      g = dist < 2.5 ? 1 : 0;
+    }
+  }
+  ghost[i] = g;
+}
+
+struct Grid {
+  int mx, my, mz, nx, ny, nz;
+};
+
+__device__ __forceinline__ Grid grid_from(const int* bbox) {
+  Grid g;
+  g.mx = bbox[0];
+  g.my = bbox[1];
+  g.mz = bbox[2];
+  g.nx = bbox[3] - bbox[0] + 1;
+  g.ny = bbox[4] - bbox[1] + 1;
+  g.nz = bbox[5] - bbox[2] + 1;
+  return g;
+}
+
+__global__ void k_bin_count(const int* __restrict__ binxyz, size_t n, const int* __restrict__ bbox,
+                            int* __restrict__ key, int* __restrict__ cnt) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Grid g = grid_from(bbox);
+  int k = ((binxyz[3 * i + 2] - g.mz) * g.ny + (binxyz[3 * i + 1] - g.my)) * g.nx + (binxyz[3 * i] - g.mx);
+  key[i] = k;
+  atomicAdd(&cnt[k], 1);
+}
+
+__global__ void k_bin_scatter(const int* __restrict__ key, size_t n, const int* __restrict__ off,
+                              int* __restrict__ cursor, int* __restrict__ cells) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int k = key[i];
+  int pos = off[k] + atomicAdd(&cursor[k], 1);
+  cells[pos] = (int)i;
+}
+
+// Sort each segment [off[s], off[s+1]) ascending (segments are short).
+__global__ void k_segment_sort(const int* __restrict__ off, size_t nseg, int* __restrict__ v) {
+  size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  int b = off[s], e = off[s + 1];
+  for (int i = b + 1; i < e; ++i) {
+    int x = v[i];
+    int j = i - 1;
+    while (j >= b && v[j] > x) {
+      v[j + 1] = v[j];
+      --j;
+    }
+    v[j + 1] = x;
+  }
+}
+
+__global__ void k_pack(CellsView c, const int* __restrict__ slot_cell, const int* __restrict__ ghost, size_t n,
+                       double* __restrict__ pk) {
+  size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int i = slot_cell[s];
+  double t[3];
+  cell_axis(c.q0[i], c.q1[i], c.q2[i], c.q3[i], t);
+  const double len = c.len[i], diam = c.diam[i];
+  // CollisionDetector::getParticleEndpoints (spatial/CollisionDetector.cpp:61-75)
+  const double half = sub(dvd(len, 2.0), dvd(diam, 2.0));
+  const double p[3] = {c.x[i], c.y[i], c.z[i]};
+  double* r = pk + s * kPack;
+  r[0] = p[0];
+  r[1] = p[1];
+  r[2] = p[2];
+  r[3] = len;
+  for (int d = 0; d < 3; ++d) {
+    double hv = mul(t[d], half);
+    r[4 + d] = sub(p[d], hv);
+    r[8 + d] = add(p[d], hv);
+    r[12 + d] = t[d];
+  }
+  r[7] = diam;
+  r[11] = (double)i;
+  r[15] = (double)ghost[i];
+}
+
+// Closest points of two segments: Eberly's branch scheme for segment-segment
+// distance (the variant the reference uses, util/SpherocylinderCell.h:64-261),
+// restated with non-contracting IEEE operations.
+__device__ void segment_closest(const double P0[3], const double P1[3], const double Q0[3], const double Q1[3],
+                                double c0[3], double c1[3], double* dist) {
+  double Pd[3], Qd[3], PQ[3];
+  for (int k = 0; k < 3; ++k) {
+    Pd[k] = sub(P1[k], P0[k]);
+    Qd[k] = sub(Q1[k], Q0[k]);
+    PQ[k] = sub(P0[k], Q0[k]);
+  }
+  const double a = dot3(Pd, Pd), b = dot3(Pd, Qd), c = dot3(Qd, Qd);
+  const double d = dot3(Pd, PQ), e = dot3(Qd, PQ);
+  const double det = sub(mul(a, c), mul(b, b));
+  double s = 0.0, t = 0.0;
+  if (det > 0.0) {
+    const double bte = mul(b, e), ctd = mul(c, d);
+    if (bte <= ctd) {
+      s = 0.0;
+      if (e <= 0.0) {
+        t = 0.0;
+        double nd = -d;
+        if (nd >= a) s = 1.0;
+        else if (nd > 0.0) s = dvd(nd, a);
+      } else if (e < c) {
+        t = dvd(e, c);
+      } else {
+        t = 1.0;
+        double bmd = sub(b, d);
+        if (bmd >= a) s = 1.0;
+        else if (bmd > 0.0) s = dvd(bmd, a);
+      }
+    } else {
+      s = sub(bte, ctd);
+      if (s >= det) {
+        s = 1.0;
+        double bpe = add(b, e);
+        if (bpe <= 0.0) {
+          t = 0.0;
+          double nd = -d;
+          if (nd <= 0.0) s = 0.0;
+          else if (nd < a) s = dvd(nd, a);
+        } else if (bpe < c) {
+          t = dvd(bpe, c);
+        } else {
+          t = 1.0;
+          double bmd = sub(b, d);
+          if (bmd <= 0.0) s = 0.0;
+          else if (bmd < a) s = dvd(bmd, a);
+        }
+      } else {
+        const double ate = mul(a, e), btd = mul(b, d);
+        if (ate <= btd) {
+          t = 0.0;
+          double nd = -d;
+          if (nd <= 0.0) s = 0.0;
+          else if (nd >= a) s = 1.0;
+          else s = dvd(nd, a);
+        } else {
+          t = sub(ate, btd);
+          if (t >= det) {
+            t = 1.0;
+            double bmd = sub(b, d);
+            if (bmd <= 0.0) s = 0.0;
+            else if (bmd >= a) s = 1.0;
+            else s = dvd(bmd, a);
+          } else {
+            s = dvd(s, det);
+            t = dvd(t, det);
+          }
+        }
+      }
+    }
+  } else {
+    if (e <= 0.0) {
+      t = 0.0;
+      double nd = -d;
+      if (nd <= 0.0) s = 0.0;
+      else if (nd >= a) s = 1.0;
+      else s = dvd(nd, a);
+    } else if (e >= c) {
+      t = 1.0;
+      double bmd = sub(b, d);
+      if (bmd <= 0.0) s = 0.0;
+      else if (bmd >= a) s = 1.0;
+      else s = dvd(bmd, a);
+    } else {
+      s = 0.0;
+      t = dvd(e, c);
+    }
+  }
+  double diff[3];
+  for (int k = 0; k < 3; ++k) {
+    c0[k] = add(P0[k], mul(Pd[k], s));
+    c1[k] = add(Q0[k], mul(Qd[k], t));
+    diff[k] = sub(c0[k], c1[k]);
+  }
+  *dist = __dsqrt_rn(dot3(diff, diff));
+}
+
+struct PairGeom {
+  double sd, n[3], cp[3], ri[3], rj[3], si, sj;
+};
+
+// tryCreateConstraint (spatial/CollisionDetector.cpp:201-311) for the pair
+// (I, J) = (A, B).  With full == false only the separation is computed.
+__device__ __forceinline__ bool pair_test(const double* __restrict__ A, const double* __restrict__ B, double tol,
+                                          bool full, PairGeom* o) {
+  const double4 a0 = *reinterpret_cast<const double4*>(A);
+  const double4 b0 = *reinterpret_cast<const double4*>(B);
+  double dv[3] = {sub(a0.x, b0.x), sub(a0.y, b0.y), sub(a0.z, b0.z)};
+  double rough = __dsqrt_rn(dot3(dv, dv));
+  if (rough > add(dvd(add(a0.w, b0.w), 2.0), tol)) return false;
+  const double4 a1 = *reinterpret_cast<const double4*>(A + 4);
+  const double4 a2 = *reinterpret_cast<const double4*>(A + 8);
+  const double4 b1 = *reinterpret_cast<const double4*>(B + 4);
+  const double4 b2 = *reinterpret_cast<const double4*>(B + 8);
+  const double P0[3] = {a1.x, a1.y, a1.z}, P1[3] = {a2.x, a2.y, a2.z};
+  const double Q0[3] = {b1.x, b1.y, b1.z}, Q1[3] = {b2.x, b2.y, b2.z};
+  double c0[3], c1[3], dist;
+  segment_closest(P0, P1, Q0, Q1, c0, c1, &dist);
+  const double sd = sub(dist, dvd(add(a1.w, b1.w), 2.0));
+  if (sd > tol) return false;
+  o->sd = sd;
+  if (!full) return true;
+  double diff[3];
+  for (int k = 0; k < 3; ++k) {
+    o->cp[k] = mul(add(c0[k], c1[k]), 0.5);
+    diff[k] = sub(c0[k], c1[k]);
+  }
+  // ArrayMath::normalize (util/ArrayMath.h:219-231)
+  const double mag = __dsqrt_rn(dot3(diff, diff));
+  if (mag > 2.220446049250313e-16) {
+    const double inv = dvd(1.0, mag);
+    for (int k = 0; k < 3; ++k) o->n[k] = mul(diff[k], inv);
+  } else {
+    o->n[0] = 1.0;
+    o->n[1] = 0.0;
+    o->n[2] = 0.0;
+  }
+  const double4 a3 = *reinterpret_cast<const double4*>(A + 12);
+  const double4 b3 = *reinterpret_cast<const double4*>(B + 12);
+  const double ta[3] = {a3.x, a3.y, a3.z}, tb[3] = {b3.x, b3.y, b3.z};
+  const double nn[3] = {-o->n[0], -o->n[1], -o->n[2]};
+  o->si = mul(0.5, fabs(dot3(o->n, ta)));
+  o->sj = mul(0.5, fabs(dot3(nn, tb)));
+  const double pa[3] = {a0.x, a0.y, a0.z}, pb[3] = {b0.x, b0.y, b0.z};
+  for (int k = 0; k < 3; ++k) {
+    o->ri[k] = sub(o->cp[k], pa[k]);
+    o->rj[k] = sub(o->cp[k], pb[k]);
+  }
+  return true;
+}
+
+// One thread per cell, cells visited in bin order.  Pass 0 counts the
+// constraints each cell emits as the smaller id of its pairs and tracks the
+// largest overlap; pass 1 writes them at the scanned offsets.
+template <bool kEmit>
+__global__ void k_pairs(const double* __restrict__ pk, const int* __restrict__ bin_off, const int* __restrict__ bbox,
+                        size_t n, double tol, int phase, int* __restrict__ cnt, const int* __restrict__ off,
+                        ConsView cs, size_t base, size_t cap, DevStatus* st) {
+  size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const Grid g = grid_from(bbox);
+  const double* A = pk + s * kPack;
+  const int a = (int)A[11];
+  // recover this cell's bin from its slot
+  int lo = 0, hi = g.nx * g.ny * g.nz;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (bin_off[mid] <= (int)s) lo = mid;
+    else hi = mid;
+  }
+  const int bx = lo % g.nx, by = (lo / g.nx) % g.ny, bz = lo / (g.nx * g.ny);
+  int count = 0;
+  double maxov = 0.0;
+  size_t w = 0;
+  if (kEmit) w = base + (size_t)off[a];
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = bz + dz;
+    if (z < 0 || z >= g.nz) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = by + dy;
+      if (y < 0 || y >= g.ny) continue;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = bx + dx;
+        if (x < 0 || x >= g.nx) continue;
+        const int bin = (z * g.ny + y) * g.nx + x;
+        const int e = bin_off[bin + 1];
+        for (int s2 = bin_off[bin]; s2 < e; ++s2) {
+          const double* B = pk + (size_t)s2 * kPack;
+          const int b = (int)B[11];
+          if (b <= a) continue;
+          PairGeom pg;
+          if (!pair_test(A, B, tol, kEmit, &pg)) continue;
+          const int copies = 1 + (B[15] != 0.0 ? 1 : 0);
+          if (!kEmit) {
+            count += copies;
+            const double ov = pg.sd < 0 ? -pg.sd : 0.0;
+            maxov = maxov < ov ? ov : maxov;
+            continue;
+          }
+          double ti[3], tj[3], nj[3] = {-pg.n[0], -pg.n[1], -pg.n[2]};
+          cross3(pg.ri, pg.n, ti);
+          cross3(pg.rj, nj, tj);
+          for (int k = 0; k < copies; ++k, ++w) {
+            if (w >= cap) {
+              raise_error(st, kDevErrCapacity, 10);
+              return;
+            }
+            cs.gi[w] = a;
+            cs.gj[w] = b;
+            cs.phase[w] = phase;
+            cs.sd[w] = pg.sd;
+            cs.gamma[w] = pg.sd >= 0.0 ? 0.0 : mul(-pg.sd, 5e2);
+            cs.nx[w] = pg.n[0];
+            cs.ny[w] = pg.n[1];
+            cs.nz[w] = pg.n[2];
+            cs.tix[w] = ti[0];
+            cs.tiy[w] = ti[1];
+            cs.tiz[w] = ti[2];
+            cs.tjx[w] = tj[0];
+            cs.tjy[w] = tj[1];
+            cs.tjz[w] = tj[2];
+            cs.rix[w] = pg.ri[0];
+            cs.riy[w] = pg.ri[1];
+            cs.riz[w] = pg.ri[2];
+            cs.rjx[w] = pg.rj[0];
+            cs.rjy[w] = pg.rj[1];
+            cs.rjz[w] = pg.rj[2];
+            cs.cpx[w] = pg.cp[0];
+            cs.cpy[w] = pg.cp[1];
+            cs.cpz[w] = pg.cp[2];
+            cs.si[w] = pg.si;
+            cs.sj[w] = pg.sj;
+          }
+        }
+      }
+    }
+  }
+  if (!kEmit) {
+    cnt[a] = count;
+    if (maxov > 0.0) atomicMax(&st->max_bits, (unsigned long long)__double_as_longlong(maxov));
+  }
+}
+
+__global__ void k_inc_count(const int* __restrict__ gi, const int* __restrict__ gj, size_t m, int* __restrict__ cnt) {
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m) return;
+  atomicAdd(&cnt[gi[c]], 1);
+  atomicAdd(&cnt[gj[c]], 1);
+}
+
+__global__ void k_inc_fill(const int* __restrict__ gi, const int* __restrict__ gj, size_t m,
+                           const int* __restrict__ off, int* __restrict__ cursor, int* __restrict__ ent) {
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m) return;
+  int a = gi[c], b = gj[c];
+  ent[off[a] + atomicAdd(&cursor[a], 1)] = (int)(2 * c);
+  ent[off[b] + atomicAdd(&cursor[b], 1)] = (int)(2 * c + 1);
+}
+
+}  // namespace
+
+cudaError_t detect_contacts(pcc_ctx* ctx, double tol, int phase, size_t* added, double* max_overlap_new) {
+  cudaStream_t s = ctx->stream;
+  const size_t n = ctx->n;
+  cudaError_t e;
+  *added = 0;
+  *max_overlap_new = 0.0;
+  if (n == 0) return cudaSuccess;
+  if ((e = ctx->bin_of.reserve(3 * n, 0, s))) return e;
+  if ((e = ctx->ghost.reserve(n, 0, s))) return e;
+  if ((e = ctx->bbox.reserve(8, 0, s))) return e;
+  static const int init[6] = {2147483647, 2147483647, 2147483647, -2147483647 - 1, -2147483647 - 1,
+                              -2147483647 - 1};
+  int* pinned = reinterpret_cast<int*>(ctx->pinned_ll);
+  cudaMemcpyAsync(ctx->bbox.p, init, sizeof init, cudaMemcpyHostToDevice, s);  // pageable: staged at once
+  k_bin<<<grid_for(n), kBlock, 0, s>>>(ctx->cells.view(), n, ctx->params.linked_cell_size, ctx->params.ghost_mode,
+                                        ctx->bin_of.p, ctx->bbox.p, ctx->ghost.p);
+  ctx->launches++;
+  cudaMemcpyAsync(pinned, ctx->bbox.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, s);
+  if ((e = cudaStreamSynchronize(s))) return e;
+  long long nx = (long long)pinned[3] - pinned[0] + 1, ny = (long long)pinned[4] - pinned[1] + 1,
+            nz = (long long)pinned[5] - pinned[2] + 1;
+  long long nbins = nx * ny * nz;
+  if (nbins <= 0 || nbins > (1LL << 30)) {
+    ctx->err = "broadphase grid too large (cells spread over more than 2^30 bins)";
+    return cudaErrorInvalidValue;
+  }
+  if ((e = ctx->bin_cnt.reserve(nbins + 1, 0, s))) return e;
+  if ((e = ctx->bin_cursor.reserve(nbins + 1, 0, s))) return e;
+  if ((e = ctx->bin_off.reserve(nbins + 1, 0, s))) return e;
+  if ((e = ctx->bin_cells.reserve(n, 0, s))) return e;
+  if ((e = ctx->cand_cnt.reserve(n + 1, 0, s))) return e;
+  if ((e = ctx->cand_off.reserve(n + 1, 0, s))) return e;
+  if ((e = ctx->pk.reserve(n * kPack, 0, s))) return e;
+  int* key = ctx->cand_cnt.p;  // reused as per-cell bin key before the pair pass
+  cudaMemsetAsync(ctx->bin_cnt.p, 0, (nbins + 1) * sizeof(int), s);
+  cudaMemsetAsync(ctx->bin_cursor.p, 0, (nbins + 1) * sizeof(int), s);
+  k_bin_count<<<grid_for(n), kBlock, 0, s>>>(ctx->bin_of.p, n, ctx->bbox.p, key, ctx->bin_cnt.p);
+  if ((e = exclusive_scan(ctx, ctx->bin_cnt.p, ctx->bin_off.p, (size_t)nbins))) return e;
+  k_bin_scatter<<<grid_for(n), kBlock, 0, s>>>(key, n, ctx->bin_off.p, ctx->bin_cursor.p, ctx->bin_cells.p);
+  k_segment_sort<<<grid_for(nbins), kBlock, 0, s>>>(ctx->bin_off.p, (size_t)nbins, ctx->bin_cells.p);
+  k_pack<<<grid_for(n), kBlock, 0, s>>>(ctx->cells.view(), ctx->bin_cells.p, ctx->ghost.p, n, ctx->pk.p);
+  ctx->launches += 4;
+  // pass 0: counts and largest overlap
+  cudaMemsetAsync(&ctx->status->max_bits, 0, sizeof(unsigned long long), s);
+  k_pairs<false><<<grid_for(n), kBlock, 0, s>>>(ctx->pk.p, ctx->bin_off.p, ctx->bbox.p, n, tol, phase,
+                                               ctx->cand_cnt.p, nullptr, ConsView{}, 0, 0, ctx->status);
+  ctx->launches++;
+  if ((e = exclusive_scan(ctx, ctx->cand_cnt.p, ctx->cand_off.p, n))) return e;
+  cudaMemcpyAsync(pinned, ctx->cand_off.p + n, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(ctx->pinned_ll + 1, &ctx->status->max_bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+  if ((e = cudaStreamSynchronize(s))) return e;
+  const size_t m = (size_t)pinned[0];
+  unsigned long long bits = (unsigned long long)ctx->pinned_ll[1];
+  double mo;
+  memcpy(&mo, &bits, sizeof mo);
+  *max_overlap_new = mo;
+  *added = m;
+  if (m == 0) return cudaSuccess;
+  if ((e = ctx->cons.reserve(ctx->ncons + m, ctx->ncons, s))) return e;
+  k_pairs<true><<<grid_for(n), kBlock, 0, s>>>(ctx->pk.p, ctx->bin_off.p, ctx->bbox.p, n, tol, phase, nullptr,
+                                              ctx->cand_off.p, ctx->cons.view(), ctx->ncons, ctx->ncons + m,
+                                              ctx->status);
+  ctx->launches++;
+  ctx->ncons += m;
+  return cudaGetLastError();
+}
+
+cudaError_t build_incidence(pcc_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  const size_t n = ctx->n, m = ctx->ncons;
+  cudaError_t e;
+  if ((e = ctx->inc_cnt.reserve(n + 1, 0, s))) return e;
+  if ((e = ctx->inc_off.reserve(n + 1, 0, s))) return e;
+  if ((e = ctx->inc_ent.reserve(2 * m + 1, 0, s))) return e;
+  if ((e = ctx->bin_cursor.reserve(n + 1, 0, s))) return e;
+  cudaMemsetAsync(ctx->inc_cnt.p, 0, (n + 1) * sizeof(int), s);
+  cudaMemsetAsync(ctx->bin_cursor.p, 0, (n + 1) * sizeof(int), s);
+  if (m) {
+    k_inc_count<<<grid_for(m), kBlock, 0, s>>>(ctx->cons.gi.p, ctx->cons.gj.p, m, ctx->inc_cnt.p);
+    ctx->launches++;
+  }
+  if ((e = exclusive_scan(ctx, ctx->inc_cnt.p, ctx->inc_off.p, n))) return e;
+  if (m) {
+    k_inc_fill<<<grid_for(m), kBlock, 0, s>>>(ctx->cons.gi.p, ctx->cons.gj.p, m, ctx->inc_off.p, ctx->bin_cursor.p,
+                                              ctx->inc_ent.p);
+    k_segment_sort<<<grid_for(n), kBlock, 0, s>>>(ctx->inc_off.p, n, ctx->inc_ent.p);
+    ctx->launches += 2;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pcc

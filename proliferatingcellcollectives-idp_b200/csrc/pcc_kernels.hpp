@@ -1,0 +1,47 @@
+// Host launchers of the device kernels (internal to libpcc_gpu.so).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pcc_ctx.hpp"
+
+namespace pcc {
+
+// ---- pcc_scan_sort.cu
+// out[i] = sum in[0..i-1] for i in [0, n]; out has n+1 entries.
+cudaError_t exclusive_scan(pcc_ctx* ctx, const int* in, int* out, size_t n);
+// Stable ascending sort of (keys, vals) by the low `bits` bits of keys;
+// keys/vals are sorted in place (scratch from ctx).
+cudaError_t radix_sort_pairs(pcc_ctx* ctx, unsigned long long* keys, int* vals, size_t n, int bits);
+
+// ---- pcc_detect.cu
+// Appends the contacts within tol of the resident cells to the constraint set
+// (ctx->ncons grows by *added).  *max_overlap_new = max(-sd, 0) over them.
+cudaError_t detect_contacts(pcc_ctx* ctx, double tol, int phase, size_t* added, double* max_overlap_new);
+// Cell -> incident constraint sides, ascending constraint index, for ctx->ncons.
+cudaError_t build_incidence(pcc_ctx* ctx);
+
+// ---- pcc_solver.cu
+// One BBPGD solve on the current constraint set (hard model).
+cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* residual, int* status);
+// Moves cells with the solver's velocities and writes back gamma / phi.
+cudaError_t apply_hard_solution(pcc_ctx* ctx, double dt);
+// Max overlap over constraints [0, ncons).
+cudaError_t max_overlap(pcc_ctx* ctx, size_t from, size_t to, double* out);
+// Soft model: Hertz forces, motion and growth parameters.
+cudaError_t soft_forces_and_move(pcc_ctx* ctx, double dt);
+// Soft model force assembly only (frozen microbench).
+cudaError_t soft_assemble(pcc_ctx* ctx);
+
+// ---- pcc_update.cu
+cudaError_t reset_ldot(pcc_ctx* ctx);
+cudaError_t grow_cells(pcc_ctx* ctx, double dt);
+// Division of every cell with len >= 2 l0, daughters appended; returns count.
+cudaError_t divide_cells(pcc_ctx* ctx, size_t* added);
+// Sort cells by x (stable) and renumber.
+cudaError_t sort_cells_by_x(pcc_ctx* ctx);
+cudaError_t colony_radius(pcc_ctx* ctx, double* out);
+cudaError_t adapt_dt(pcc_ctx* ctx);  // updates ctx->params.dt
+cudaError_t mobility(pcc_ctx* ctx);
+
+}  // namespace pcc

@@ -1,0 +1,708 @@
+// Hard-model BBPGD solver and soft-model force assembly (sm_100a).
+//
+// The BBPGD solve (solver/BBPGD.cpp:32-127 with the gradient of
+// dynamics/models/hard/HardModelGradient.cpp:89-158) runs as ONE persistent
+// cooperative kernel per ReLCP phase.  Each iteration is two grid-wide passes:
+//   pass A, one thread per cell: F = D^T (gamma - gamma_old) and
+//     sigma = L^T gamma gathered over the cell's incidence list (ascending
+//     constraint order, no atomics), U = M F, growth rate and its change;
+//   pass B, one thread per constraint: phi_next = Phi + dt D U - dt L dldot,
+//     the projected-gradient residual and the three Barzilai-Borwein dot
+//     products, reduced per fixed chunk of constraints.
+// The projection gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0) is recomputed
+// where it is needed (both passes), so no extra pass stores it.  The last block
+// to reach a barrier reduces the chunk partials in a fixed order and publishes
+// alpha and the convergence decision: results do not depend on the grid size
+// or on which block arrives last.  Barrier waits are bounded; a wait that runs
+// out raises kDevErrTimeout and the kernel returns.
+#include <cfloat>
+#include <cmath>
+
+#include "pcc_kernels.hpp"
+
+namespace pcc {
+
+namespace {
+
+constexpr int kChunk = 1024;            // constraints per reduction chunk
+constexpr int kPerThread = kChunk / kBlock;
+constexpr long long kSpinLimit = 1LL << 26;
+
+struct SolverArgs {
+  // constraints
+  long long m;
+  const int *gi, *gj;
+  const double *nx, *ny, *nz, *tix, *tiy, *tiz, *tjx, *tjy, *tjz, *si, *sj;
+  double *phi;    // Phi on entry; phi_next of the returned iterate on exit
+  double *gamma;  // gamma_0 on entry (also gamma_old); gamma_{k-1} on exit
+  double *gam[2], *g[2];
+  // cells
+  long long n;
+  const int *inc_off, *inc_ent;
+  const double *Mlin, *Mrot, *len, *ldot_prev;
+  double *U, *dl, *F, *sig, *ldot, *imp;
+  double dt, lambda, tau, tol;
+  long long max_it;
+  double* partials;  // 4 per chunk
+  long long nchunks;
+  SolverScalars* sc;
+  DevStatus* st;
+};
+
+// gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0): VecWAXPY with PETSc's special
+// cases for the coefficient, then VecPointwiseMax against 0.
+__device__ __forceinline__ double project(double gp, double g, double alpha) {
+  const double a = -alpha;
+  double v;
+  if (a == 1.0) v = add(gp, g);
+  else if (a == -1.0) v = sub(gp, g);
+  else if (a == 0.0) v = gp;
+  else v = add(mul(a, g), gp);
+  return v < 0.0 ? 0.0 : v;
+}
+
+// VecScale(x, a) for one entry.
+__device__ __forceinline__ double vscale(double a, double x) {
+  if (a == 1.0) return x;
+  if (a == 0.0) return 0.0;
+  return mul(a, x);
+}
+
+__device__ __forceinline__ bool barrier(SolverScalars* sc, unsigned nblocks, DevStatus* st) {
+  __shared__ unsigned s_gen;
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_ok = 1;
+    s_gen = *(volatile unsigned*)&sc->gen;
+    __threadfence();
+    unsigned t = atomicAdd(&sc->count, 1u);
+    if (t == nblocks - 1) {
+      sc->count = 0;
+      __threadfence();
+      atomicAdd(&sc->gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*(volatile unsigned*)&sc->gen == s_gen) {
+        __nanosleep(40);
+        if (++spins > kSpinLimit) {
+          raise_error(st, kDevErrTimeout, 20);
+          s_ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+// Barrier whose last arriving block first runs `reduce` (all its threads).
+template <typename R>
+__device__ __forceinline__ bool barrier_reduce(SolverScalars* sc, unsigned nblocks, DevStatus* st, R reduce) {
+  __shared__ unsigned s_gen;
+  __shared__ int s_last, s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_ok = 1;
+    s_gen = *(volatile unsigned*)&sc->gen;
+    __threadfence();
+    unsigned t = atomicAdd(&sc->count, 1u);
+    s_last = (t == nblocks - 1);
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    reduce();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sc->count = 0;
+      __threadfence();
+      atomicAdd(&sc->gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    long long spins = 0;
+    while (*(volatile unsigned*)&sc->gen == s_gen) {
+      __nanosleep(40);
+      if (++spins > kSpinLimit) {
+        raise_error(st, kDevErrTimeout, 21);
+        s_ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+// Pass A for cell p.  mode 0: gamma = gamma_0; mode 1: gamma_k projected from
+// (gam_prev, g_prev, alpha).  Writes U and dldot; with `final` also F, sigma,
+// ldot and impedance.
+__device__ __forceinline__ void cell_pass(const SolverArgs& a, long long p, int mode, const double* gprev_gam,
+                                          const double* gprev_g, double alpha, bool final) {
+  double F[6] = {0, 0, 0, 0, 0, 0};
+  double sg = 0.0;
+  const int b = a.inc_off[p], e = a.inc_off[p + 1];
+  for (int k = b; k < e; ++k) {
+    const int ent = a.inc_ent[k];
+    const long long c = ent >> 1;
+    const int side = ent & 1;
+    const double gold = a.gamma[c];
+    const double gc = mode == 0 ? gold : project(ldcg(gprev_gam + c), ldcg(gprev_g + c), alpha);
+    const double diff = sub(gc, gold);
+    double D[6];
+    if (side == 0) {
+      D[0] = a.nx[c];
+      D[1] = a.ny[c];
+      D[2] = a.nz[c];
+      D[3] = a.tix[c];
+      D[4] = a.tiy[c];
+      D[5] = a.tiz[c];
+    } else {
+      D[0] = -a.nx[c];
+      D[1] = -a.ny[c];
+      D[2] = -a.nz[c];
+      D[3] = a.tjx[c];
+      D[4] = a.tjy[c];
+      D[5] = a.tjz[c];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) F[q] = add(F[q], mul(D[q], diff));
+    sg = add(sg, mul(side == 0 ? a.si[c] : a.sj[c], gc));
+  }
+  const double ml = a.Mlin[p], mr = a.Mrot[p];
+  double* U = a.U + 6 * p;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const double uc = add(0.0, mul(q < 3 ? ml : mr, F[q]));
+    U[q] = add(uc, 0.0);  // + U_ext (zero: no Brownian kicks)
+  }
+  double im = exp(vscale(-a.lambda, sg));
+  double ld = vscale(dvd(1.0, a.tau), mul(a.len[p], im));
+  a.dl[p] = sub(ld, a.ldot_prev[p]);
+  if (final) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) a.F[6 * p + q] = F[q];
+    a.sig[p] = sg;
+    a.ldot[p] = ld;
+    a.imp[p] = im;
+  }
+}
+
+// Pass B value for constraint c: phi_next(gamma) given U and dldot.
+__device__ __forceinline__ double constraint_grad(const SolverArgs& a, long long c) {
+  const int i = a.gi[c], j = a.gj[c];
+  const double* Ui = a.U + 6 * (long long)i;
+  const double* Uj = a.U + 6 * (long long)j;
+  const double Di[6] = {a.nx[c], a.ny[c], a.nz[c], a.tix[c], a.tiy[c], a.tiz[c]};
+  const double Dj[6] = {-a.nx[c], -a.ny[c], -a.nz[c], a.tjx[c], a.tjy[c], a.tjz[c]};
+  double pd = 0.0;
+  // MatMult row c: ascending columns; gi < gj for every emitted constraint
+  if (i < j) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) pd = add(pd, mul(Di[q], ldcg(Ui + q)));
+#pragma unroll
+    for (int q = 0; q < 6; ++q) pd = add(pd, mul(Dj[q], ldcg(Uj + q)));
+  } else {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) pd = add(pd, mul(Dj[q], ldcg(Uj + q)));
+#pragma unroll
+    for (int q = 0; q < 6; ++q) pd = add(pd, mul(Di[q], ldcg(Ui + q)));
+  }
+  double gr = 0.0;
+  if (i < j) {
+    gr = add(gr, mul(a.si[c], ldcg(a.dl + i)));
+    gr = add(gr, mul(a.sj[c], ldcg(a.dl + j)));
+  } else {
+    gr = add(gr, mul(a.sj[c], ldcg(a.dl + j)));
+    gr = add(gr, mul(a.si[c], ldcg(a.dl + i)));
+  }
+  // VecMAXPY(phi_next, {dt, -dt}, {phidot, growth})
+  return add(a.phi[c], add(mul(a.dt, pd), mul(-a.dt, gr)));
+}
+
+__device__ __forceinline__ double proj_grad_abs(double g, double gam) {
+  double v = gam > 0 ? g : (g < 0.0 ? g : 0.0);
+  return fabs(v);
+}
+
+// Fixed-shape block reduction of 4 values (sum, sum, sum, max).
+__device__ __forceinline__ void block_reduce4(double v[4], double* sm) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) sm[q * kBlock + t] = v[q];
+  __syncthreads();
+  for (int w = kBlock / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      sm[t] = add(sm[t], sm[t + w]);
+      sm[kBlock + t] = add(sm[kBlock + t], sm[kBlock + t + w]);
+      sm[2 * kBlock + t] = add(sm[2 * kBlock + t], sm[2 * kBlock + t + w]);
+      double x = sm[3 * kBlock + t], y = sm[3 * kBlock + t + w];
+      sm[3 * kBlock + t] = x < y ? y : x;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = sm[q * kBlock];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
+  __shared__ double sm[4 * kBlock];
+  const unsigned nb = gridDim.x;
+  const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
+  const long long stride = (long long)nb * kBlock;
+  SolverScalars* sc = a.sc;
+
+  // ---- gradient at gamma_0 and the initial residual (BBPGD.cpp:40-44)
+  for (long long p = tid; p < a.n; p += stride) cell_pass(a, p, 0, nullptr, nullptr, 0.0, false);
+  if (!barrier(sc, nb, a.st)) return;
+  for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
+    double v[4] = {0, 0, 0, 0};
+    for (int k = 0; k < kPerThread; ++k) {
+      long long c = ch * kChunk + k * kBlock + threadIdx.x;
+      if (c >= a.m) break;
+      double g = constraint_grad(a, c);
+      double gm = a.gamma[c];
+      a.g[0][c] = g;
+      a.gam[0][c] = gm;
+      double r = proj_grad_abs(g, gm);
+      v[3] = v[3] < r ? r : v[3];
+    }
+    block_reduce4(v, sm);
+    if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
+  }
+  auto reduce_init = [&]() {
+    double v[4] = {0, 0, 0, 0};
+    for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
+      double r = ldcg(a.partials + 4 * ch + 3);
+      v[3] = v[3] < r ? r : v[3];
+    }
+    block_reduce4(v, sm);
+    if (threadIdx.x == 0) {
+      sc->res0 = v[3];
+      sc->residual = v[3];
+      sc->alpha = 1.0 / v[3];
+      sc->converged = 0;
+    }
+  };
+  if (!barrier_reduce(sc, nb, a.st, reduce_init)) return;
+
+  int p = 0;  // buffer of gamma_{k-1}, g_{k-1}
+  long long it = 1;
+  while (it < a.max_it) {
+    const double alpha = *(volatile double*)&sc->alpha;
+    const bool check = (it % 10) == 0;
+    const double* gp = a.gam[p];
+    const double* gg = a.g[p];
+    double* gc_out = a.gam[1 - p];
+    double* g_out = a.g[1 - p];
+    for (long long q = tid; q < a.n; q += stride) cell_pass(a, q, 1, gp, gg, alpha, check);
+    if (!barrier(sc, nb, a.st)) return;
+    for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
+      double v[4] = {0, 0, 0, 0};  // sum dgam^2, sum dgam*dg, sum dg^2, max residual
+      for (int k = 0; k < kPerThread; ++k) {
+        long long c = ch * kChunk + k * kBlock + threadIdx.x;
+        if (c >= a.m) break;
+        const double gpc = ldcg(gp + c), ggc = ldcg(gg + c);
+        const double gam = project(gpc, ggc, alpha);
+        const double g = constraint_grad(a, c);
+        gc_out[c] = gam;
+        g_out[c] = g;
+        const double dgm = sub(gam, gpc), dg = sub(g, ggc);
+        v[0] = add(v[0], mul(dgm, dgm));
+        v[1] = add(v[1], mul(dgm, dg));
+        v[2] = add(v[2], mul(dg, dg));
+        if (check) {
+          double r = proj_grad_abs(g, gam);
+          v[3] = v[3] < r ? r : v[3];
+        }
+      }
+      block_reduce4(v, sm);
+      if (threadIdx.x == 0) {
+        a.partials[4 * ch + 0] = v[0];
+        a.partials[4 * ch + 1] = v[1];
+        a.partials[4 * ch + 2] = v[2];
+        a.partials[4 * ch + 3] = v[3];
+      }
+    }
+    auto reduce_iter = [&]() {
+      double v[4] = {0, 0, 0, 0};
+      for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
+        v[0] = add(v[0], ldcg(a.partials + 4 * ch + 0));
+        v[1] = add(v[1], ldcg(a.partials + 4 * ch + 1));
+        v[2] = add(v[2], ldcg(a.partials + 4 * ch + 2));
+        double r = ldcg(a.partials + 4 * ch + 3);
+        v[3] = v[3] < r ? r : v[3];
+      }
+      block_reduce4(v, sm);
+      if (threadIdx.x == 0) {
+        int conv = 0;
+        if (check) {
+          sc->residual = v[3];
+          if (v[3] <= a.tol) conv = 1;
+        }
+        if (!conv) {
+          // BB1 on even, BB2 on odd iterations (BBPGD.cpp:98-112)
+          double num, den;
+          if (it % 2 == 0) {
+            num = v[0];
+            den = v[1];
+          } else {
+            den = v[2];
+            num = v[1];
+          }
+          if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
+          sc->alpha = dvd(num, den);
+        }
+        sc->converged = conv;
+        sc->iterations = it;
+      }
+    };
+    if (!barrier_reduce(sc, nb, a.st, reduce_iter)) return;
+    if (*(volatile int*)&sc->converged) break;
+    p = 1 - p;
+    ++it;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->iterations = it;
+  if (!*(volatile int*)&sc->converged) return;
+  // Returned result (Hard.cpp:170 with BBPGD.cpp:124): gamma_{k-1}, phi(gamma_k).
+  for (long long c = tid; c < a.m; c += stride) {
+    a.gamma[c] = ldcg(a.gam[p] + c);
+    a.phi[c] = ldcg(a.g[1 - p] + c);
+  }
+}
+
+// Cell update after a solve: dC = G U (Physics.cpp:220-265), Euler step and
+// quaternion normalisation (simulation/Particle.cpp:37-57, 110-120), force,
+// velocity and growth parameters (ParticleManager.cpp:29-130).
+__global__ void k_move(CellsView c, long long n, const double* __restrict__ U, const double* __restrict__ F,
+                       const double* __restrict__ ldot, const double* __restrict__ imp, const double* __restrict__ sig,
+                       double dt) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double s = c.q0[i], wx = c.q1[i], wy = c.q2[i], wz = c.q3[i];
+  const double* u = U + 6 * i;
+  double dC[7];
+  for (int k = 0; k < 3; ++k) dC[k] = add(0.0, mul(1.0, u[k]));
+  const double xi[4][3] = {{mul(-0.5, wx), mul(-0.5, wy), mul(-0.5, wz)},
+                           {mul(0.5, s), mul(-0.5, wz), mul(0.5, wy)},
+                           {mul(0.5, wz), mul(0.5, s), mul(-0.5, wx)},
+                           {mul(-0.5, wy), mul(0.5, wx), mul(0.5, s)}};
+  for (int r = 0; r < 4; ++r) {
+    double acc = 0.0;
+    for (int k = 0; k < 3; ++k) acc = add(acc, mul(xi[r][k], u[3 + k]));
+    dC[3 + r] = acc;
+  }
+  c.x[i] = add(c.x[i], mul(dt, dC[0]));
+  c.y[i] = add(c.y[i], mul(dt, dC[1]));
+  c.z[i] = add(c.z[i], mul(dt, dC[2]));
+  double q[4] = {add(s, mul(dt, dC[3])), add(wx, mul(dt, dC[4])), add(wy, mul(dt, dC[5])), add(wz, mul(dt, dC[6]))};
+  double nrm = __dsqrt_rn(add(add(add(mul(q[0], q[0]), mul(q[1], q[1])), mul(q[2], q[2])), mul(q[3], q[3])));
+  c.q0[i] = dvd(q[0], nrm);
+  c.q1[i] = dvd(q[1], nrm);
+  c.q2[i] = dvd(q[2], nrm);
+  c.q3[i] = dvd(q[3], nrm);
+  for (int k = 0; k < 6; ++k) {
+    c.force[6 * i + k] = F[6 * i + k];
+    c.vel[6 * i + k] = u[k];
+  }
+  c.ldot[i] = ldot[i];
+  c.imp[i] = imp[i];
+  c.stress[i] = sig[i];
+}
+
+__global__ void k_max_overlap(const double* __restrict__ sd, long long from, long long to, DevStatus* st) {
+  long long c = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (c < to) v = sd[c] < 0 ? -sd[c] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) {
+    double w = __shfl_down_sync(0xffffffffu, v, o);
+    v = v < w ? w : v;
+  }
+  if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(&st->max_bits, (unsigned long long)__double_as_longlong(v));
+}
+
+// x^1.5 correctly rounded in practice: sqrt with its exact residual and the
+// exact error of the product (error-free transformations), one final rounding.
+__device__ __forceinline__ double pow15(double x) {
+  const double s = __dsqrt_rn(x);
+  const double r = fma(-s, s, x);           // x - s^2, exact
+  const double ds = r / (2.0 * s);          // sqrt(x) ~ s + ds
+  const double p = x * s;
+  const double pe = fma(x, s, -p);          // x*s - p, exact
+  return p + (pe + x * ds);
+}
+
+// Soft model, per contact: Hertz force magnitude (dynamics/models/Soft.cpp:46-60)
+__global__ void k_soft_fel(ConsView cs, long long m, const double* __restrict__ diam, double kcc,
+                           double* __restrict__ fel) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m) return;
+  const double overlap = -cs.sd[c];
+  if (overlap <= 0.00) {
+    fel[c] = 0.0;
+    return;
+  }
+  const double R1 = dvd(diam[cs.gi[c]], 2.0), R2 = dvd(diam[cs.gj[c]], 2.0);
+  const double R_eff = __dsqrt_rn(dvd(mul(R1, R2), add(R1, R2)));
+  fel[c] = mul(mul(R_eff, kcc), pow15(overlap));
+}
+
+// Soft model, per cell: force, torque and stress gathered over the incident
+// contacts in ascending contact order (the order of the VecSetValues ADD
+// stream for that cell), then U = M F, dC = G U and the move, growth rate.
+__global__ void k_soft_cell(CellsView c, long long n, ConsView cs, const int* __restrict__ inc_off,
+                            const int* __restrict__ inc_ent, const double* __restrict__ fel, double xi, double lambda,
+                            double tau, double dt, int move) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double F[6] = {0, 0, 0, 0, 0, 0};
+  double sg = 0.0;
+  for (int k = inc_off[i]; k < inc_off[i + 1]; ++k) {
+    const int ent = inc_ent[k];
+    const long long q = ent >> 1;
+    if (-cs.sd[q] <= 0.00) continue;  // Soft.cpp:49 skips non-overlapping contacts
+    const double fe = fel[q];
+    const double fi[3] = {mul(cs.nx[q], fe), mul(cs.ny[q], fe), mul(cs.nz[q], fe)};
+    double f[3], r[3], t[3];
+    if ((ent & 1) == 0) {
+      f[0] = fi[0];
+      f[1] = fi[1];
+      f[2] = fi[2];
+      r[0] = cs.rix[q];
+      r[1] = cs.riy[q];
+      r[2] = cs.riz[q];
+    } else {
+      f[0] = -fi[0];
+      f[1] = -fi[1];
+      f[2] = -fi[2];
+      r[0] = cs.rjx[q];
+      r[1] = cs.rjy[q];
+      r[2] = cs.rjz[q];
+    }
+    cross3(r, f, t);
+    for (int d = 0; d < 3; ++d) F[d] = add(F[d], f[d]);
+    for (int d = 0; d < 3; ++d) F[3 + d] = add(F[3 + d], t[d]);
+    sg = add(sg, mul((ent & 1) == 0 ? cs.si[q] : cs.sj[q], fe));
+  }
+  if (!move) {
+    for (int d = 0; d < 6; ++d) c.force[6 * i + d] = F[d];
+    c.stress[i] = sg;
+    return;
+  }
+  // Mobility (Physics.cpp:192-218)
+  const double l = c.len[i];
+  const double ml = dvd(1.0, mul(l, xi));
+  const double mr = dvd(12.0, mul(mul(mul(l, l), l), xi));
+  double u[6];
+  for (int d = 0; d < 6; ++d) u[d] = add(add(0.0, mul(d < 3 ? ml : mr, F[d])), 0.0);
+  const double s = c.q0[i], wx = c.q1[i], wy = c.q2[i], wz = c.q3[i];
+  double dC[7];
+  for (int k = 0; k < 3; ++k) dC[k] = add(0.0, mul(1.0, u[k]));
+  const double xm[4][3] = {{mul(-0.5, wx), mul(-0.5, wy), mul(-0.5, wz)},
+                           {mul(0.5, s), mul(-0.5, wz), mul(0.5, wy)},
+                           {mul(0.5, wz), mul(0.5, s), mul(-0.5, wx)},
+                           {mul(-0.5, wy), mul(0.5, wx), mul(0.5, s)}};
+  for (int rr = 0; rr < 4; ++rr) {
+    double acc = 0.0;
+    for (int k = 0; k < 3; ++k) acc = add(acc, mul(xm[rr][k], u[3 + k]));
+    dC[3 + rr] = acc;
+  }
+  c.x[i] = add(c.x[i], mul(dt, dC[0]));
+  c.y[i] = add(c.y[i], mul(dt, dC[1]));
+  c.z[i] = add(c.z[i], mul(dt, dC[2]));
+  double qq[4] = {add(s, mul(dt, dC[3])), add(wx, mul(dt, dC[4])), add(wy, mul(dt, dC[5])), add(wz, mul(dt, dC[6]))};
+  double nrm = __dsqrt_rn(add(add(add(mul(qq[0], qq[0]), mul(qq[1], qq[1])), mul(qq[2], qq[2])), mul(qq[3], qq[3])));
+  c.q0[i] = dvd(qq[0], nrm);
+  c.q1[i] = dvd(qq[1], nrm);
+  c.q2[i] = dvd(qq[2], nrm);
+  c.q3[i] = dvd(qq[3], nrm);
+  for (int d = 0; d < 6; ++d) {
+    c.force[6 * i + d] = F[d];
+    c.vel[6 * i + d] = u[d];
+  }
+  // calculate_growth_rate_vector (HardModelGradient.cpp:43-52)
+  const double im = exp(vscale(-lambda, sg));
+  c.stress[i] = sg;
+  c.imp[i] = im;
+  c.ldot[i] = vscale(dvd(1.0, tau), mul(l, im));
+}
+
+__global__ void k_mobility(const double* __restrict__ len, long long n, double xi, double* __restrict__ Ml,
+                           double* __restrict__ Mr) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double l = len[i];
+  Ml[i] = dvd(1.0, mul(l, xi));
+  Mr[i] = dvd(12.0, mul(mul(mul(l, l), l), xi));
+}
+
+}  // namespace
+
+cudaError_t mobility(pcc_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  if ((e = ctx->Mlin.reserve(ctx->n + 1, 0, s))) return e;
+  if ((e = ctx->Mrot.reserve(ctx->n + 1, 0, s))) return e;
+  if (ctx->n) {
+    k_mobility<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.len.p, (long long)ctx->n, ctx->params.xi,
+                                                   ctx->Mlin.p, ctx->Mrot.p);
+    ctx->launches++;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* residual, int* status) {
+  cudaStream_t s = ctx->stream;
+  const size_t n = ctx->n, m = ctx->ncons;
+  cudaError_t e;
+  const size_t mm = m + 1, nn = n + 1;
+  if ((e = ctx->gam_a.reserve(mm, 0, s)) || (e = ctx->gam_b.reserve(mm, 0, s)) || (e = ctx->g_a.reserve(mm, 0, s)) ||
+      (e = ctx->g_b.reserve(mm, 0, s)))
+    return e;
+  if ((e = ctx->U.reserve(6 * nn, 0, s)) || (e = ctx->dldot.reserve(nn, 0, s)) || (e = ctx->F.reserve(6 * nn, 0, s)) ||
+      (e = ctx->sig.reserve(nn, 0, s)) || (e = ctx->ldot_new.reserve(nn, 0, s)) || (e = ctx->imp_new.reserve(nn, 0, s)))
+    return e;
+  const long long nchunks = (long long)((m + kChunk - 1) / kChunk);
+  if ((e = ctx->partials.reserve(4 * (nchunks + 1), 0, s))) return e;
+  if ((e = ctx->scal.reserve(1, 0, s))) return e;
+  cudaMemsetAsync(ctx->scal.p, 0, sizeof(SolverScalars), s);
+
+  SolverArgs a;
+  ConsView cv = ctx->cons.view();
+  a.m = (long long)m;
+  a.gi = cv.gi;
+  a.gj = cv.gj;
+  a.nx = cv.nx;
+  a.ny = cv.ny;
+  a.nz = cv.nz;
+  a.tix = cv.tix;
+  a.tiy = cv.tiy;
+  a.tiz = cv.tiz;
+  a.tjx = cv.tjx;
+  a.tjy = cv.tjy;
+  a.tjz = cv.tjz;
+  a.si = cv.si;
+  a.sj = cv.sj;
+  a.phi = cv.sd;
+  a.gamma = cv.gamma;
+  a.gam[0] = ctx->gam_a.p;
+  a.gam[1] = ctx->gam_b.p;
+  a.g[0] = ctx->g_a.p;
+  a.g[1] = ctx->g_b.p;
+  a.n = (long long)n;
+  a.inc_off = ctx->inc_off.p;
+  a.inc_ent = ctx->inc_ent.p;
+  a.Mlin = ctx->Mlin.p;
+  a.Mrot = ctx->Mrot.p;
+  a.len = ctx->cells.len.p;
+  a.ldot_prev = ctx->cells.ldot.p;
+  a.U = ctx->U.p;
+  a.dl = ctx->dldot.p;
+  a.F = ctx->F.p;
+  a.sig = ctx->sig.p;
+  a.ldot = ctx->ldot_new.p;
+  a.imp = ctx->imp_new.p;
+  a.dt = dt;
+  a.lambda = ctx->params.lambda;
+  a.tau = ctx->params.tau;
+  a.tol = ctx->params.tolerance;
+  a.max_it = ctx->params.max_bbpgd_iterations;
+  a.partials = ctx->partials.p;
+  a.nchunks = nchunks;
+  a.sc = ctx->scal.p;
+  a.st = ctx->status;
+
+  if (ctx->coop_blocks == 0) {
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bbpgd, kBlock, 0))) return e;
+    ctx->coop_blocks = per_sm * ctx->num_sms;
+  }
+  long long want = (long long)grid_for((long long)n);
+  if (nchunks > want) want = nchunks;
+  if (want > ctx->coop_blocks) want = ctx->coop_blocks;
+  if (want < 1) want = 1;
+  void* args[] = {&a};
+  e = cudaLaunchCooperativeKernel((void*)k_bbpgd, dim3((unsigned)want), dim3(kBlock), args, 0, s);
+  ctx->launches++;
+  if (e) return e;
+  SolverScalars host;
+  if ((e = cudaMemcpyAsync(&host, ctx->scal.p, sizeof host, cudaMemcpyDeviceToHost, s))) return e;
+  if ((e = cudaMemcpyAsync(ctx->status_host, ctx->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s))) return e;
+  if ((e = cudaStreamSynchronize(s))) return e;
+  *iterations = host.iterations;
+  *residual = host.residual;
+  if (ctx->status_host->flags) {
+    *status = (ctx->status_host->flags & kDevErrTimeout) ? PCC_ERR_TIMEOUT : PCC_ERR_BOUNDS;
+  } else {
+    *status = host.converged ? PCC_OK : PCC_ERR_NOCONV_BBPGD;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t apply_hard_solution(pcc_ctx* ctx, double dt) {
+  if (!ctx->n) return cudaSuccess;
+  k_move<<<grid_for(ctx->n), kBlock, 0, ctx->stream>>>(ctx->cells.view(), (long long)ctx->n, ctx->U.p, ctx->F.p,
+                                                       ctx->ldot_new.p, ctx->imp_new.p, ctx->sig.p, dt);
+  ctx->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t max_overlap(pcc_ctx* ctx, size_t from, size_t to, double* out) {
+  cudaStream_t s = ctx->stream;
+  cudaMemsetAsync(&ctx->status->max_bits, 0, sizeof(unsigned long long), s);
+  if (to > from) {
+    k_max_overlap<<<grid_for((long long)(to - from)), kBlock, 0, s>>>(ctx->cons.sd.p, (long long)from, (long long)to,
+                                                                     ctx->status);
+    ctx->launches++;
+  }
+  cudaMemcpyAsync(ctx->pinned_ll, &ctx->status->max_bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e) return e;
+  unsigned long long b = (unsigned long long)ctx->pinned_ll[0];
+  memcpy(out, &b, sizeof(double));
+  return cudaSuccess;
+}
+
+cudaError_t soft_assemble(pcc_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  const size_t m = ctx->ncons;
+  if ((e = ctx->fel.reserve(m + 1, 0, s))) return e;
+  if (m) {
+    k_soft_fel<<<grid_for(m), kBlock, 0, s>>>(ctx->cons.view(), (long long)m, ctx->cells.diam.p, ctx->params.kcc,
+                                              ctx->fel.p);
+    ctx->launches++;
+  }
+  if (ctx->n) {
+    k_soft_cell<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.view(), (long long)ctx->n, ctx->cons.view(),
+                                                    ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p, ctx->params.xi,
+                                                    ctx->params.lambda, ctx->params.tau, 0.0, 0);
+    ctx->launches++;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t soft_forces_and_move(pcc_ctx* ctx, double dt) {
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  const size_t m = ctx->ncons;
+  if ((e = ctx->fel.reserve(m + 1, 0, s))) return e;
+  if (m) {
+    k_soft_fel<<<grid_for(m), kBlock, 0, s>>>(ctx->cons.view(), (long long)m, ctx->cells.diam.p, ctx->params.kcc,
+                                              ctx->fel.p);
+    ctx->launches++;
+  }
+  if (ctx->n) {
+    k_soft_cell<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.view(), (long long)ctx->n, ctx->cons.view(),
+                                                    ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p, ctx->params.xi,
+                                                    ctx->params.lambda, ctx->params.tau, dt, 1);
+    ctx->launches++;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pcc

@@ -1,0 +1,191 @@
+"""Host binding of the device library (libpcc_gpu.so) through its C ABI.
+
+`Colony` is the Python face of one pcc_ctx: one colony resident on one GPU.
+Its methods follow the reference's step interface -- `solve` is
+ParticleManager::step (solveHardModel / solveSoftPotential), `step` is one
+iteration of Domain::run -- and raise RuntimeError with the reference's
+messages when the C ABI returns an error status.  There is no CPU fallback:
+if the library is missing or no GPU is visible, construction fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+from . import abi
+
+LIB_PATH = Path(__file__).resolve().parent / "libpcc_gpu.so"
+_LIB = None
+
+
+def load_library(path: str | os.PathLike | None = None):
+    """Load libpcc_gpu.so (built by build.py).  Raises if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build the CUDA library first (python -c 'import __graft_entry__ as g; g.build()')")
+    lib = C.CDLL(str(p))
+    P = C.POINTER
+    VP = C.c_void_p
+    lib.pcc_default_params.argtypes = [P(abi.Params)]
+    lib.pcc_create.argtypes = [P(abi.Params), C.c_int, P(VP)]
+    lib.pcc_destroy.argtypes = [VP]
+    lib.pcc_last_error.restype = C.c_char_p
+    lib.pcc_last_error.argtypes = [VP]
+    lib.pcc_set_dt.argtypes = [VP, C.c_double]
+    lib.pcc_get_dt.argtypes = [VP, P(C.c_double)]
+    lib.pcc_upload_cells.argtypes = [VP, P(abi.Cells), C.c_size_t]
+    lib.pcc_download_cells.argtypes = [VP, P(abi.Cells), C.c_size_t, P(C.c_size_t)]
+    lib.pcc_cell_count.argtypes = [VP, P(C.c_size_t)]
+    lib.pcc_solve.argtypes = [VP, C.c_double, C.c_int, P(abi.StepStats)]
+    lib.pcc_step.argtypes = [VP, P(abi.StepStats)]
+    lib.pcc_run.argtypes = [VP, C.c_double, C.c_longlong, P(C.c_longlong), P(C.c_double), P(abi.StepStats)]
+    lib.pcc_detect_contacts.argtypes = [VP, C.c_double, C.c_int, P(abi.Contacts), C.c_size_t, P(C.c_size_t)]
+    lib.pcc_get_constraints.argtypes = [VP, P(abi.Contacts), C.c_size_t, P(C.c_size_t)]
+    lib.pcc_bbpgd_frozen.argtypes = [VP, C.c_double, C.c_int, P(C.c_longlong), P(C.c_double), P(C.c_float)]
+    lib.pcc_soft_forces_frozen.argtypes = [VP, C.c_int, P(C.c_float)]
+    lib.pcc_get_stream.restype = VP
+    lib.pcc_get_stream.argtypes = [VP]
+    lib.pcc_launch_count.restype = C.c_longlong
+    lib.pcc_launch_count.argtypes = [VP]
+    lib.pcc_division_seed.restype = C.c_uint
+    lib.pcc_division_seed.argtypes = [C.c_ulonglong, C.c_ulonglong]
+    lib.pcc_division_length_host.restype = C.c_double
+    lib.pcc_division_length_host.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_double]
+    _LIB = lib
+    return lib
+
+
+# Messages the reference raises for the same conditions.
+_REFERENCE_MESSAGES = {
+    abi.PCC_ERR_NOCONV_BBPGD: "BBPGD did not converge",
+    abi.PCC_ERR_NOCONV_RELCP: "Maximum number of constraint iterations reached",
+}
+
+
+class PccError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(msg)
+        self.status = status
+
+
+class Colony:
+    """One colony resident on one GPU (a pcc_ctx)."""
+
+    def __init__(self, params: abi.Params, device: int = 0):
+        self.lib = load_library()
+        self.h = C.c_void_p()
+        rc = self.lib.pcc_create(C.byref(params), device, C.byref(self.h))
+        if rc != 0:
+            raise PccError(rc, f"pcc_create failed: {abi.STATUS_NAMES.get(rc, rc)}")
+        self.n_cells_hint = 1024
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.pcc_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.lib.pcc_last_error(self.h)
+            msg = msg.decode() if msg else ""
+            raise PccError(rc, _REFERENCE_MESSAGES.get(rc, f"{what}: {abi.STATUS_NAMES.get(rc, rc)}: {msg}"))
+
+    # state transfer
+    def set_cells(self, cells: dict):
+        ca = abi.CellArrays.from_dict(cells)
+        self._check(self.lib.pcc_upload_cells(self.h, C.byref(ca.struct), len(cells["x"])), "upload")
+
+    def upload(self, ca: abi.CellArrays, n: int):
+        self._check(self.lib.pcc_upload_cells(self.h, C.byref(ca.struct), n), "upload")
+
+    def download(self, ca: abi.CellArrays) -> int:
+        n = C.c_size_t(0)
+        self._check(self.lib.pcc_download_cells(self.h, C.byref(ca.struct), ca.cap, C.byref(n)), "download")
+        return int(n.value)
+
+    @property
+    def n_cells(self) -> int:
+        n = C.c_size_t(0)
+        self._check(self.lib.pcc_cell_count(self.h, C.byref(n)), "count")
+        return int(n.value)
+
+    def get_cells(self) -> dict:
+        n = self.n_cells
+        ca = abi.CellArrays(n)
+        self.download(ca)
+        return ca.to_dict(n)
+
+    # solver / driver
+    def solve(self, dt: float, it: int = 0) -> dict:
+        st = abi.StepStats()
+        self._check(self.lib.pcc_solve(self.h, dt, it, C.byref(st)), "solve")
+        return st.as_dict()
+
+    def step(self) -> dict:
+        st = abi.StepStats()
+        self._check(self.lib.pcc_step(self.h, C.byref(st)), "step")
+        return st.as_dict()
+
+    def run(self, end_radius: float, max_steps: int):
+        steps = C.c_longlong(0)
+        cs = C.c_double(0)
+        st = abi.StepStats()
+        self._check(self.lib.pcc_run(self.h, end_radius, max_steps, C.byref(steps), C.byref(cs), C.byref(st)), "run")
+        return int(steps.value), float(cs.value), st.as_dict()
+
+    def _contacts(self, fn, *args) -> dict:
+        n = C.c_size_t(0)
+        self._check(fn(self.h, *args, None, 0, C.byref(n)), "contacts")
+        ca = abi.ContactArrays(int(n.value))
+        self._check(fn(self.h, *args, C.byref(ca.struct), ca.cap, C.byref(n)), "contacts")
+        return ca.to_dict(int(n.value))
+
+    def detect(self, tol: float, phase: int = 0) -> dict:
+        return self._contacts(self.lib.pcc_detect_contacts, C.c_double(tol), C.c_int(phase))
+
+    def constraints(self) -> dict:
+        return self._contacts(self.lib.pcc_get_constraints)
+
+    def bbpgd_frozen(self, dt: float, repeats: int = 1):
+        it = C.c_longlong(0)
+        res = C.c_double(0)
+        ms = C.c_float(0)
+        self._check(self.lib.pcc_bbpgd_frozen(self.h, dt, repeats, C.byref(it), C.byref(res), C.byref(ms)), "bbpgd")
+        return int(it.value), float(res.value), float(ms.value)
+
+    def soft_forces_frozen(self, repeats: int = 1) -> float:
+        ms = C.c_float(0)
+        self._check(self.lib.pcc_soft_forces_frozen(self.h, repeats, C.byref(ms)), "soft")
+        return float(ms.value)
+
+    @property
+    def dt(self) -> float:
+        v = C.c_double(0)
+        self._check(self.lib.pcc_get_dt(self.h, C.byref(v)), "dt")
+        return v.value
+
+    @dt.setter
+    def dt(self, v: float):
+        self._check(self.lib.pcc_set_dt(self.h, v), "dt")
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.pcc_get_stream(self.h) or 0)
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.pcc_launch_count(self.h))
+
+
+def division_length(seed: int, k: int, length: float) -> float:
+    return load_library().pcc_division_length_host(seed, k, length)

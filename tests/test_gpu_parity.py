@@ -1,0 +1,178 @@
+"""Parity of the device library (through its C ABI) with the reference.
+
+Inputs are the golden snapshots made by the reference's own code
+(tests/golden/make_golden.py) and the plain-C oracle where a case is built on
+the fly.  Tolerances, and why:
+  * contact detection: bit-exact (same binning, same IEEE operations, no FMA);
+  * soft model, one call: positions within 1e-12 absolute -- the per-cell
+    force sums add the same terms in a different order;
+  * hard model: the device reduces the BBPGD dot products in a different order
+    (fixed-chunk trees instead of one sequential sum), so iterates differ by
+    rounding and the solver may stop at a different multiple of 10
+    iterations.  Both stop at residual <= tolerance, so positions agree to the
+    solver tolerance: 1e-6 absolute after one call at tolerance 1e-3 (the
+    iterates agree to rounding there), 2 x tolerance at tolerance 1e-6 (18,000
+    BB iterations amplify rounding to the residual level), 5e-3 after 3000
+    steps of growth (trajectories of a contact-driven colony are chaotic),
+    and both runs satisfy the LCP (gamma >= 0, max overlap <= tolerance).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import cells_max_diff, load_fixture, normalized_contacts, params_of, sub
+from oracles import OracleColony
+from pcc_b200 import abi
+from pcc_b200.device import Colony, PccError
+
+pytestmark = pytest.mark.gpu
+
+SNAPSHOTS = ["hard_r10_seed3", "hard_r5_seed0_noghost", "soft_r3_seed1"]
+
+
+@pytest.mark.parametrize("name", SNAPSHOTS)
+@pytest.mark.parametrize("tag,tol", [("det25_", 0.25), ("dettol_", 1e-3), ("det0_", 0.0)])
+def test_contacts_bit_exact(name, tag, tol):
+    fx = load_fixture(name)
+    g = Colony(params_of(fx))
+    g.set_cells(sub(fx, "cells_"))
+    got = normalized_contacts(g.detect(tol, 0))
+    want = normalized_contacts(sub(fx, tag))
+    assert got["gid_i"].size == want["gid_i"].size
+    for k in want:
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+
+
+def test_contacts_bit_exact_without_ghost_copies():
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx, ghost_mode=abi.GHOSTS_NONE)
+    g, o = Colony(p), OracleColony(p)
+    g.set_cells(sub(fx, "cells_"))
+    o.set_cells(sub(fx, "cells_"))
+    a, b = normalized_contacts(g.detect(0.25)), normalized_contacts(o.detect(0.25))
+    for k in b:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert a["gid_i"].size < load_fixture("hard_r10_seed3")["det25_sd"].size  # ghosts add duplicates
+
+
+def test_soft_solve_matches_reference():
+    fx = load_fixture("soft_on_hard_r10_seed3")
+    p = params_of(fx)
+    g = Colony(p)
+    g.set_cells(sub(fx, "cells_"))
+    st = g.solve(p.dt, 0)
+    want = fx["solve_stats"][0]
+    assert st["n_constraints"] == want["n_constraints"]
+    assert st["max_overlap"] == want["max_overlap"]
+    got, ref = g.get_cells(), sub(fx, "solve_cells_")
+    d = cells_max_diff(got, ref)
+    assert max(d.values()) < 1e-12, d
+    np.testing.assert_allclose(got["force"], ref["force"], rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(got["stress"], ref["stress"], rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(got["ldot"], ref["ldot"], rtol=1e-14)
+
+
+@pytest.mark.parametrize("name,pos_tol", [("hard_r10_seed3", 1e-6), ("hard_tight_r10_seed3", 2e-6),
+                                          ("hard_r5_seed0_noghost", 1e-6)])
+def test_hard_solve_matches_reference(name, pos_tol):
+    fx = load_fixture(name)
+    p = params_of(fx)
+    g = Colony(p)
+    g.set_cells(sub(fx, "cells_"))
+    st = g.solve(p.dt, 0)
+    want = fx["solve_stats"][0]
+    assert st["residual"] <= p.tolerance and st["max_overlap"] <= p.tolerance or st["relcp_iterations"] > 0
+    assert abs(st["relcp_iterations"] - want["relcp_iterations"]) <= 1
+    d = cells_max_diff(g.get_cells(), sub(fx, "solve_cells_"))
+    assert max(d.values()) < pos_tol, (d, st, want)
+    cons = g.constraints()
+    assert np.all(cons["gamma"] >= 0.0)
+
+
+def test_single_cell_growth_bit_exact_and_ten_iterations():
+    p = abi.default_params(dt=1e-3, fixed_dt=1)
+    g, o = Colony(p), OracleColony(p)
+    g.set_cells(abi.seed_cell(0))
+    o.set_cells(abi.seed_cell(0))
+    for _ in range(700):
+        sg, so = g.step(), o.step()
+        assert sg["bbpgd_iterations"] == so["bbpgd_iterations"]
+        assert sg["n_cells"] == so["n_cells"]
+    assert sg["n_cells"] == 2
+    d = cells_max_diff(g.get_cells(), o.get_cells())
+    assert max(d.values()) == 0.0, d
+
+
+def test_empty_colony_steps():
+    g = Colony(abi.default_params(dt=1e-3, fixed_dt=1))
+    g.set_cells({k: [] for k in abi.seed_cell(0)})
+    st = g.step()
+    assert st["n_cells"] == 0 and st["n_constraints"] == 0
+
+
+def test_division_matches_oracle():
+    """Five separated cells at division length: daughters, ages and draws
+    follow the reference's divide (simulation/Particle.cpp:122-150)."""
+    cells = {k: [] for k in abi.seed_cell(0)}
+    for i in range(5):
+        c = abi.seed_cell(100 + i)
+        c["x"] = [10.0 * i]
+        c["y"] = [3.0 * (i % 2)]
+        c["length"] = [2.0]
+        for k in cells:
+            cells[k] += c[k]
+    p = abi.default_params(dt=1e-3, fixed_dt=1, seed=42)
+    g, o = Colony(p), OracleColony(p)
+    g.set_cells(cells)
+    o.set_cells(cells)
+    sg, so = g.step(), o.step()
+    assert sg["n_divided"] == so["n_divided"] == 5
+    assert sg["n_cells"] == so["n_cells"] == 10
+    a, b = g.get_cells(), o.get_cells()
+    np.testing.assert_array_equal(a["age"], b["age"])
+    d = cells_max_diff(a, b)
+    assert max(d.values()) < 1e-12, d
+
+
+def test_trajectory_matches_reference():
+    fx = load_fixture("traj_hard_seed3_3000")
+    p = params_of(fx)
+    g = Colony(p)
+    g.set_cells(sub(fx, "start_"))
+    hist = [g.step() for _ in range(len(fx["hist_n_cells"]))]
+    np.testing.assert_array_equal([h["n_cells"] for h in hist], fx["hist_n_cells"])
+    assert all(h["max_overlap"] <= p.tolerance for h in hist)
+    d = cells_max_diff(g.get_cells(), sub(fx, "final_"))
+    assert max(d.values()) < 5e-3, d
+
+
+def test_solve_is_deterministic():
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx)
+    out = []
+    for _ in range(2):
+        g = Colony(p)
+        g.set_cells(sub(fx, "cells_"))
+        g.solve(p.dt, 0)
+        out.append(g.get_cells())
+    d = cells_max_diff(out[0], out[1], keys=("x", "y", "q0", "q3", "length", "ldot", "stress"))
+    assert max(d.values()) == 0.0, d
+
+
+def test_bbpgd_nonconvergence_raises_reference_message():
+    fx = load_fixture("hard_r10_seed3")
+    g = Colony(params_of(fx, max_bbpgd_iterations=5))
+    g.set_cells(sub(fx, "cells_"))
+    with pytest.raises(PccError, match="BBPGD did not converge") as e:
+        g.solve(1e-3, 0)
+    assert e.value.status == abi.PCC_ERR_NOCONV_BBPGD
+
+
+def test_relcp_exhaustion_raises_reference_message():
+    fx = load_fixture("hard_r10_seed3")
+    g = Colony(params_of(fx, max_recursive_iterations=1))
+    g.set_cells(sub(fx, "cells_"))
+    with pytest.raises(PccError, match="Maximum number of constraint iterations reached") as e:
+        g.solve(1e-3, 0)
+    assert e.value.status == abi.PCC_ERR_NOCONV_RELCP
