@@ -1,0 +1,358 @@
+"""Benchmark of the collision hot path: cell-steps/s of the hard model.
+
+Workload (default): one colony of radius 260 in the hard model, FP64, the
+scale of the reference's largest published run (R = 260).  The colony is a
+synthetic, deterministic dense packing (pcc_b200.synth.dense_colony: ~2.2e5
+rod cells in orientation domains, every neighbour touching), since growing a
+real one takes hours; a step is one full simulator step on it through the C
+ABI -- divide, x-sort renumbering, the ReLCP loop of contact detection and
+BBPGD solves, motion, growth and the CFL time-step adaptation (dt starts at
+3e-4, capped at 1e-3).  value = sum of cells over the K timed steps / device
+time (CUDA events on the library's stream), summed over ranks; each rank runs
+its own colony (replicas, no collective on the data path: weak scaling).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference simulator's own C++ code (compiled in
+place against single-rank PETSc/MPI stand-ins, oracle/_ref/libpccref_fast.so,
+release flags) on a bounded sample of the same workload on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+import pcc_pkg  # noqa: E402
+
+pcc_pkg.load_package()
+from pcc_b200 import abi, synth  # noqa: E402
+
+METRIC = "cell-steps/s to R_end; served colonies/s, p50/p99 vs plain GPU at same LCP tol"
+UNIT = "cell-steps/s"
+RADIUS = 260.0
+CPU_SAMPLE_RADIUS = 40.0  # bounded sample for the CPU legs (~5e3 cells)
+
+
+def colony_params(**over) -> abi.Params:
+    return abi.default_params(dt=3e-4, fixed_dt=0, dt_cap=1e-3, mode=abi.MODE_HARD,
+                              ghost_mode=abi.GHOSTS_SINGLE_RANK, seed=0, **over)
+
+
+def make_colony(radius: float, seed: int) -> dict:
+    return synth.dense_colony(radius, seed=seed, lane_gap=0.0, end_gap=0.0)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+def traffic_ratio() -> float | None:
+    """DRAM bytes / algorithmic bytes of the BBPGD kernel from the committed ncu
+    summary (profiles/k_bbpgd_*.md, line 'dram_to_algorithmic: <ratio>')."""
+    for f in sorted((ROOT / "profiles").glob("k_bbpgd_*.md")):
+        m = re.search(r"dram_to_algorithmic:\s*([0-9.eE+-]+)", f.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reduce_max(world: int, v: float) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(world: int, v: float) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def aggregate(cells_per_rank: list[float], ms_per_rank: list[float]) -> tuple[float, float]:
+    """Whole-job throughput: all ranks' cell-steps over the slowest rank's time."""
+    t = max(ms_per_rank)
+    return sum(cells_per_rank) / (t / 1e3), t
+
+
+def cpu_rate(fast_ref: bool, seconds: float = 15.0, radius: float = CPU_SAMPLE_RADIUS, min_steps: int = 2,
+             max_steps: int | None = None, warmup: int = 1):
+    """cell-steps/s of a CPU implementation on a bounded sample of the workload."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracles import OracleColony, RefColony
+    kind = "port"
+    p = colony_params()
+    col = None
+    if fast_ref and (ROOT / "oracle" / "_ref" / "libpccref_fast.so").exists():
+        col = RefColony(p, fast=True)
+        kind = "reference"
+    else:
+        col = OracleColony(p)
+    cells = make_colony(radius, seed=0)
+    col.set_cells(cells)
+    for _ in range(warmup):
+        col.step()
+    t0 = time.perf_counter()
+    cs, k = 0.0, 0
+    while (time.perf_counter() - t0 < seconds or k < min_steps) and (max_steps is None or k < max_steps):
+        cs += col.step()["n_cells"]
+        k += 1
+    el = time.perf_counter() - t0
+    return cs / el, kind, k, len(cells["x"]), el
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    rate, kind, k, n, el = cpu_rate(True, seconds=1e9, min_steps=args.steps, max_steps=args.steps,
+                                    warmup=args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "hard model colony step, FP64 (bounded sample)", "radius": CPU_SAMPLE_RADIUS,
+                   "cells": n, "parallelism": "1 rank, 1 thread"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
+                         "sample": f"{k} steps of the synthetic dense colony at R={CPU_SAMPLE_RADIUS:g} "
+                                   f"({n} cells) after {args.warmup} warm-up steps"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    world, rank, local = dist_setup()
+    from pcc_b200 import build, device
+    if rank == 0:
+        build.build()
+    barrier(world)
+    import torch
+    torch.cuda.init()
+    cells = make_colony(args.radius, seed=rank)
+    p = colony_params(capacity_hint=int(len(cells["x"]) * 1.5))
+    col = device.Colony(p, device=local)
+    col.set_cells(cells)
+    stream = torch.cuda.ExternalStream(col.stream, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        col.step()
+    col.profiling(True)
+    launches0 = col.launches
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hist = []
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            hist.append(col.step())
+            if args.verbose:
+                print(json.dumps(hist[-1]), file=sys.stderr, flush=True)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    launches = col.launches - launches0
+    prof = col.profile()
+    cells_steps = float(sum(h["n_cells"] for h in hist))
+    ms_max = reduce_max(world, ms)
+    total = reduce_sum(world, cells_steps)
+    value = total / (ms_max / 1e3)
+
+    # end to end through the C ABI with host buffers: upload the state from
+    # pinned host memory, step, read the state back, every step
+    n_cap = int(hist[-1]["n_cells"] * 1.3) + 16
+    host = {f: torch.empty(n_cap, dtype=torch.float64, pin_memory=True) for f in abi.CELL_FIELDS}
+    host["age"] = torch.empty(n_cap, dtype=torch.int32, pin_memory=True)
+    host["force"] = torch.empty(6 * n_cap, dtype=torch.float64, pin_memory=True)
+    host["velocity"] = torch.empty(6 * n_cap, dtype=torch.float64, pin_memory=True)
+    import ctypes as C
+    cs = abi.Cells()
+    for f in abi.CELL_FIELDS + ("force", "velocity"):
+        setattr(cs, f, C.cast(host[f].data_ptr(), C.POINTER(C.c_double)))
+    cs.age = C.cast(host["age"].data_ptr(), C.POINTER(C.c_int))
+
+    class Pinned:
+        struct = cs
+        cap = n_cap
+
+    n = col.download(Pinned)
+    per_cell_bytes = 8 * len(abi.CELL_FIELDS) + 4 + 8 * 12
+    h2d = d2h = 0
+    e2e_cells = 0.0
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    e2e_steps = max(1, args.steps)
+    for _ in range(e2e_steps):
+        col.upload(Pinned, n)
+        h2d += n * per_cell_bytes
+        st = col.step()
+        e2e_cells += st["n_cells"]
+        n = col.download(Pinned)
+        d2h += n * per_cell_bytes
+    t1.record(stream)
+    t1.synchronize()
+    barrier(world)
+    e2e_ms = reduce_max(world, t0.elapsed_time(t1))
+    e2e_total = reduce_sum(world, e2e_cells)
+    e2e_value = e2e_total / (e2e_ms / 1e3)
+
+    peaks = measured_peaks()
+    bb_ms = prof["bbpgd_ms"]
+    achieved = prof["bbpgd_algo_bytes"] / (bb_ms / 1e3) / 1e9 if bb_ms > 0 else 0.0
+    ratio = traffic_ratio()
+    launches_bb = max(prof["bbpgd_launches"], 1)
+    traffic = ratio * prof["bbpgd_algo_bytes"] / launches_bb if ratio else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"hard model colony step, FP64, synthetic dense colony R={args.radius:g}",
+                   "cells_per_rank": int(hist[0]["n_cells"]), "ghost_mode": "single_rank",
+                   "tolerance": p.tolerance, "dt_start": 3e-4, "dt_cap": 1e-3,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state + constraints > 126 MB per step)"},
+        "roofline": {"bound": "hbm", "achieved": achieved,
+                     "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
+                     "traffic": traffic, "kernel": "k_bbpgd (persistent BBPGD)",
+                     "peak_source": "fallback" if peaks.get("fallback") else "measured"},
+        "bbpgd_iterations_per_s": prof["bbpgd_iterations"] / (ms / 1e3),
+        "bbpgd_iterations_per_step": prof["bbpgd_iterations"] / max(args.steps, 1),
+        "stage_ms": {"bbpgd": bb_ms, "detect": prof["detect_ms"], "solve": prof["solve_ms"], "total": ms},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
+                "d2h_bytes_per_step": d2h // e2e_steps},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, kind, k, ncpu, el = cpu_rate(True)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
+                                "sample": f"{k} steps ({el:.1f} s) of the synthetic dense colony at "
+                                          f"R={CPU_SAMPLE_RADIUS:g} ({ncpu} cells); smaller colonies need "
+                                          f"fewer BBPGD iterations per cell, so this favours the CPU"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    col.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--radius", type=float, default=RADIUS)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--verbose", action="store_true", help="per-step solver statistics on stderr")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

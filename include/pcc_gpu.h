@@ -133,6 +133,19 @@ typedef struct pcc_step_stats {
   double sim_time;              /* after the step */
 } pcc_step_stats;
 
+/* Device-time accounting of the last pcc_reset_profile .. now window
+ * (CUDA events on the context's stream; only while profiling is on). */
+typedef struct pcc_profile {
+  long long bbpgd_launches;     /* persistent BBPGD kernel launches */
+  long long bbpgd_iterations;   /* iterations they ran */
+  double bbpgd_ms;              /* device time of those launches */
+  double bbpgd_algo_bytes;      /* sum over launches of iterations * (312 C + 288 N) */
+  double detect_ms;             /* contact detection + incidence lists */
+  double solve_ms;              /* whole pcc_solve calls */
+  long long solves;
+  double cell_solves;           /* sum of cell counts over solves */
+} pcc_profile;
+
 typedef struct pcc_ctx pcc_ctx;
 
 /* Reference defaults (CLIParser.h:296-365): hard mode, temperature 0, ghost
@@ -181,6 +194,11 @@ pcc_status pcc_soft_forces_frozen(pcc_ctx* ctx, int repeats, float* ms_per_assem
 
 /* The CUDA stream all work of the context is queued on (a cudaStream_t). */
 void* pcc_get_stream(const pcc_ctx* ctx);
+
+/* Stage timing with CUDA events (off by default; adds no host syncs). */
+pcc_status pcc_set_profiling(pcc_ctx* ctx, int on);
+pcc_status pcc_reset_profile(pcc_ctx* ctx);
+pcc_status pcc_get_profile(const pcc_ctx* ctx, pcc_profile* out);
 
 /* Kernel launches issued by this context so far (for launch accounting). */
 long long pcc_launch_count(const pcc_ctx* ctx);

@@ -91,6 +91,22 @@ class StepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Profile(C.Structure):
+    _fields_ = [
+        ("bbpgd_launches", C.c_longlong),
+        ("bbpgd_iterations", C.c_longlong),
+        ("bbpgd_ms", C.c_double),
+        ("bbpgd_algo_bytes", C.c_double),
+        ("detect_ms", C.c_double),
+        ("solve_ms", C.c_double),
+        ("solves", C.c_longlong),
+        ("cell_solves", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def default_params(**over) -> Params:
     """Reference defaults (code/cpp/src/util/CLIParser.h:296-365), hard mode."""
     p = Params()

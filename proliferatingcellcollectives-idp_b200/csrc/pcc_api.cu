@@ -113,6 +113,16 @@ pcc_status check_device(pcc_ctx* ctx, const char* where) {
   return fail(ctx, PCC_ERR_BOUNDS, buf);
 }
 
+// Adds the device time since ev[2] to the detection account.
+void profile_detect(pcc_ctx* ctx) {
+  if (!ctx->profiling) return;
+  cudaEventRecord(ctx->ev[3], ctx->stream);
+  cudaEventSynchronize(ctx->ev[3]);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+  ctx->prof.detect_ms += ms;
+}
+
 #define CU(call, where)                                  \
   do {                                                   \
     cudaError_t e_ = (call);                             \
@@ -132,10 +142,15 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
     double ov_old = 0.0, ov_new = 0.0;
     if (before) CU(max_overlap(ctx, 0, before, &ov_old), "max_overlap");
     size_t added = 0;
+    if (ctx->profiling) cudaEventRecord(ctx->ev[2], ctx->stream);
     CU(detect_contacts(ctx, phase == 0 ? .25 : tol, phase, &added, &ov_new), "detect");
     max_ov = ov_old < ov_new ? ov_new : ov_old;
-    if (max_ov <= tol && phase > 0) break;
+    if (max_ov <= tol && phase > 0) {
+      profile_detect(ctx);
+      break;
+    }
     CU(build_incidence(ctx), "incidence");
+    profile_detect(ctx);
     long long it = 0;
     int status = 0;
     CU(bbpgd_solve(ctx, dt, &it, &res, &status), "bbpgd");
@@ -169,8 +184,10 @@ pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
   CU(reset_ldot(ctx), "reset");
   size_t added = 0;
   double max_ov = 0.0;
+  if (ctx->profiling) cudaEventRecord(ctx->ev[2], ctx->stream);
   CU(detect_contacts(ctx, 0.0, 0, &added, &max_ov), "detect");
   CU(build_incidence(ctx), "incidence");
+  profile_detect(ctx);
   CU(soft_forces_and_move(ctx, dt), "soft");
   CU(grow_cells(ctx, dt), "grow");
   pcc_status rc = check_device(ctx, "soft step");
@@ -274,6 +291,8 @@ pcc_status pcc_destroy(pcc_ctx* ctx) {
   if (!ctx) return PCC_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->status) cudaFree(ctx->status);
   if (ctx->status_host) cudaFreeHost(ctx->status_host);
   if (ctx->pinned_ll) cudaFreeHost(ctx->pinned_ll);
@@ -384,8 +403,18 @@ pcc_status pcc_solve(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* out) {
   cudaSetDevice(ctx->device);
   pcc_step_stats st;
   std::memset(&st, 0, sizeof st);
+  if (ctx->profiling) cudaEventRecord(ctx->ev[4], ctx->stream);
   pcc_status rc = ctx->params.mode == PCC_MODE_SOFT ? solve_soft(ctx, dt, &st) : solve_hard(ctx, dt, &st);
   st.dt_used = dt;
+  if (ctx->profiling) {
+    cudaEventRecord(ctx->ev[5], ctx->stream);
+    cudaEventSynchronize(ctx->ev[5]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+    ctx->prof.solve_ms += ms;
+    ctx->prof.solves++;
+    ctx->prof.cell_solves += (double)st.n_cells;
+  }
   if (out) *out = st;
   return rc;
 }
@@ -547,6 +576,28 @@ pcc_status pcc_soft_forces_frozen(pcc_ctx* ctx, int repeats, float* ms_per_assem
   cudaEventDestroy(b);
   if (ms_per_assembly) *ms_per_assembly = ms / repeats;
   return check_device(ctx, "soft_frozen");
+}
+
+pcc_status pcc_set_profiling(pcc_ctx* ctx, int on) {
+  if (!ctx) return PCC_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (on && !ctx->ev[0]) {
+    for (auto& e : ctx->ev) CU(cudaEventCreate(&e), "profiling");
+  }
+  ctx->profiling = on != 0;
+  return PCC_OK;
+}
+
+pcc_status pcc_reset_profile(pcc_ctx* ctx) {
+  if (!ctx) return PCC_ERR_INVALID;
+  std::memset(&ctx->prof, 0, sizeof ctx->prof);
+  return PCC_OK;
+}
+
+pcc_status pcc_get_profile(const pcc_ctx* ctx, pcc_profile* out) {
+  if (!ctx || !out) return PCC_ERR_INVALID;
+  *out = ctx->prof;
+  return PCC_OK;
 }
 
 void* pcc_get_stream(const pcc_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

@@ -74,10 +74,6 @@ struct SolverScalars {
   double res0;          // initial residual
 };
 
-struct Timers {
-  double detect_ms = 0, solve_ms = 0, update_ms = 0;
-};
-
 }  // namespace pcc
 
 struct pcc_ctx {
@@ -129,5 +125,7 @@ struct pcc_ctx {
   long long launches = 0;
   int coop_blocks = 0;  // co-resident blocks of the solver kernel
 
-  pcc::Timers timers;
+  bool profiling = false;
+  pcc_profile prof{};
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };

@@ -626,15 +626,25 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   if (want > ctx->coop_blocks) want = ctx->coop_blocks;
   if (want < 1) want = 1;
   void* args[] = {&a};
+  if (ctx->profiling) cudaEventRecord(ctx->ev[0], s);
   e = cudaLaunchCooperativeKernel((void*)k_bbpgd, dim3((unsigned)want), dim3(kBlock), args, 0, s);
   ctx->launches++;
   if (e) return e;
+  if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);
   SolverScalars host;
   if ((e = cudaMemcpyAsync(&host, ctx->scal.p, sizeof host, cudaMemcpyDeviceToHost, s))) return e;
   if ((e = cudaMemcpyAsync(ctx->status_host, ctx->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s))) return e;
   if ((e = cudaStreamSynchronize(s))) return e;
   *iterations = host.iterations;
   *residual = host.residual;
+  if (ctx->profiling) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    ctx->prof.bbpgd_launches++;
+    ctx->prof.bbpgd_iterations += host.iterations;
+    ctx->prof.bbpgd_ms += ms;
+    ctx->prof.bbpgd_algo_bytes += (double)host.iterations * (312.0 * (double)m + 288.0 * (double)n);
+  }
   if (ctx->status_host->flags) {
     *status = (ctx->status_host->flags & kDevErrTimeout) ? PCC_ERR_TIMEOUT : PCC_ERR_BOUNDS;
   } else {

@@ -47,6 +47,9 @@ def load_library(path: str | os.PathLike | None = None):
     lib.pcc_get_constraints.argtypes = [VP, P(abi.Contacts), C.c_size_t, P(C.c_size_t)]
     lib.pcc_bbpgd_frozen.argtypes = [VP, C.c_double, C.c_int, P(C.c_longlong), P(C.c_double), P(C.c_float)]
     lib.pcc_soft_forces_frozen.argtypes = [VP, C.c_int, P(C.c_float)]
+    lib.pcc_set_profiling.argtypes = [VP, C.c_int]
+    lib.pcc_reset_profile.argtypes = [VP]
+    lib.pcc_get_profile.argtypes = [VP, P(abi.Profile)]
     lib.pcc_get_stream.restype = VP
     lib.pcc_get_stream.argtypes = [VP]
     lib.pcc_launch_count.restype = C.c_longlong
@@ -177,6 +180,15 @@ class Colony:
     @dt.setter
     def dt(self, v: float):
         self._check(self.lib.pcc_set_dt(self.h, v), "dt")
+
+    def profiling(self, on: bool = True):
+        self._check(self.lib.pcc_set_profiling(self.h, 1 if on else 0), "profiling")
+        self._check(self.lib.pcc_reset_profile(self.h), "profiling")
+
+    def profile(self) -> dict:
+        pr = abi.Profile()
+        self._check(self.lib.pcc_get_profile(self.h, C.byref(pr)), "profile")
+        return pr.as_dict()
 
     @property
     def stream(self) -> int:
