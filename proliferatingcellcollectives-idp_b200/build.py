@@ -31,8 +31,26 @@ def needs_build() -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+CLI = PKG / "pcc_cellcollectives"
+
+
+def build_cli(verbose: bool = False) -> Path:
+    """The C++ command-line driver over the C ABI (links libpcc_gpu.so)."""
+    src = PKG / "host" / "pcc_cellcollectives.cpp"
+    deps = [src, PKG / "host" / "pcc_adapter.hpp", ROOT / "include" / "pcc_gpu.h", OUT]
+    if CLI.exists() and all(d.stat().st_mtime <= CLI.stat().st_mtime for d in deps):
+        return CLI
+    cmd = ["g++", "-std=c++17", "-O2", f"-I{ROOT / 'include'}", f"-I{PKG / 'host'}", "-o", str(CLI), str(src),
+           f"-L{PKG}", "-lpcc_gpu", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return CLI
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
+        build_cli(verbose)
         return OUT
     cmd = [nvcc(), *NVCC_FLAGS, f"-I{ROOT / 'include'}", f"-I{PKG / 'csrc'}", "-o", str(OUT) + ".tmp",
            *[str(PKG / "csrc" / s) for s in SOURCES]]
@@ -40,6 +58,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
     os.replace(str(OUT) + ".tmp", OUT)
+    build_cli(verbose)
     return OUT
 
 
