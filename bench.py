@@ -338,6 +338,28 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_frozen(args):
+    """BBPGD microbench on a frozen state: after W warm-up steps, detect the
+    phase-0 contacts once and time `--steps` solves of that constraint set
+    (the captured launch of the committed ncu summaries)."""
+    from pcc_b200 import device
+    cells = make_colony(args.radius, seed=0)
+    col = device.Colony(colony_params(capacity_hint=int(len(cells["x"]) * 1.5)))
+    col.set_cells(cells)
+    for _ in range(args.warmup):
+        col.step()
+    n = col.n_cells
+    col.profiling(True)
+    it, res, ms = col.bbpgd_frozen(3e-4, max(args.steps, 1))
+    prof = col.profile()
+    m = int(round((prof["bbpgd_algo_bytes"] / max(prof["bbpgd_iterations"], 1) - 288.0 * n) / 312.0))
+    algo = it * (312.0 * m + 288.0 * n)
+    print(json.dumps({"frozen_bbpgd": True, "radius": args.radius, "cells": n, "constraints": m, "iterations": it,
+                      "residual": res, "ms_per_solve": ms, "algo_bytes_per_solve": algo,
+                      "algo_gbs": algo / (ms / 1e3) / 1e9,
+                      "frac_of_hbm": algo / (ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -347,8 +369,11 @@ def main():
     ap.add_argument("--radius", type=float, default=RADIUS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--verbose", action="store_true", help="per-step solver statistics on stderr")
+    ap.add_argument("--frozen", action="store_true", help="BBPGD microbench on a frozen constraint set")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.frozen:
+        run_frozen(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

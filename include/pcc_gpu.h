@@ -93,7 +93,15 @@ typedef struct pcc_params {
   unsigned long long seed;             /* seeds the division length draws */
   int precision;                       /* PCC_PRECISION_FP64 */
   long long capacity_hint;             /* expected peak cell count (0: grow on demand) */
+  int solver_variant;                  /* PCC_SOLVER_AUTO or PCC_SOLVER_GENERAL */
 } pcc_params;
+
+/* BBPGD kernel choice.  A planar colony (every z = 0, rotation about z only)
+ * keeps those zeros exactly through a step, so the planar form -- which skips
+ * the terms that are exact zeros -- gives bit-identical results with half the
+ * memory traffic.  AUTO picks it whenever the colony is planar. */
+#define PCC_SOLVER_AUTO 0
+#define PCC_SOLVER_GENERAL 1
 
 /* Host SoA view of n cells (index = global id after the x-sort).  Optional
  * arrays may be NULL.  force/velocity hold 6 values per cell (linear, angular). */

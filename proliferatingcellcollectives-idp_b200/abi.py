@@ -30,6 +30,8 @@ MODE_HARD = 0
 MODE_SOFT = 1
 GHOSTS_NONE = 0
 GHOSTS_SINGLE_RANK = 1
+SOLVER_AUTO = 0
+SOLVER_GENERAL = 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -58,6 +60,7 @@ class Params(C.Structure):
         ("seed", C.c_ulonglong),
         ("precision", C.c_int),
         ("capacity_hint", C.c_longlong),
+        ("solver_variant", C.c_int),
     ]
 
 
@@ -131,6 +134,7 @@ def default_params(**over) -> Params:
     p.seed = 0
     p.precision = 0
     p.capacity_hint = 0
+    p.solver_variant = 0
     for k, v in over.items():
         if k == "lambda":
             k = "lambda_"

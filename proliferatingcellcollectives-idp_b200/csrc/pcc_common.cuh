@@ -93,6 +93,12 @@ template <typename T>
 __device__ __forceinline__ T ldcg(const T* p) {
   return __ldcg(p);
 }
+template <>
+__device__ __forceinline__ double4 ldcg<double4>(const double4* p) {
+  const double2 lo = __ldcg(reinterpret_cast<const double2*>(p));
+  const double2 hi = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
 
 __device__ __forceinline__ void raise_error(DevStatus* st, unsigned flag, int where) {
   atomicOr(&st->flags, flag);

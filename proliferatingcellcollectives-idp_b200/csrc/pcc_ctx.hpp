@@ -106,6 +106,11 @@ struct pcc_ctx {
   pcc::DevBuf<double> partials;
   pcc::DevBuf<pcc::SolverScalars> scal;
   pcc::DevBuf<double> fel;  // soft: Hertz force magnitude per contact
+  // packed operands of the planar solver
+  pcc::DevBuf<int2> p_ij;
+  pcc::DevBuf<double2> p_n, p_t, p_s;
+  pcc::DevBuf<double4> p_st0, p_st1, p_inc, p_cell, p_u;
+  bool planar = false;  // set by the last binning pass
 
   // step scratch
   pcc::DevBuf<int> div_flag, div_off;
@@ -123,7 +128,8 @@ struct pcc_ctx {
   long long iter = 0;
   double sim_time = 0, radius = 0;
   long long launches = 0;
-  int coop_blocks = 0;  // co-resident blocks of the solver kernel
+  int coop_blocks = 0;         // co-resident blocks of the general solver kernel
+  int coop_blocks_planar = 0;  // ... of the planar one
 
   bool profiling = false;
   pcc_profile prof{};

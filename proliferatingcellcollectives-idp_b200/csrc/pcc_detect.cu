@@ -40,6 +40,8 @@ __global__ void k_bin(CellsView c, size_t n, double h, int ghost_mode, int* __re
   atomicMax(&bbox[3], bx);
   atomicMax(&bbox[4], by);
   atomicMax(&bbox[5], bz);
+  // planar colony (z = 0, rotation about z only): the solver may use its 2D form
+  if (z != 0.0 || c.q1[i] != 0.0 || c.q2[i] != 0.0) atomicOr(&bbox[6], 1);
   int g = 0;
   if (ghost_mode == PCC_GHOSTS_SINGLE_RANK) {
     // Domain::exchangeGhostParticles at world size 1 (spatial/Domain.cpp:339-403)
@@ -415,15 +417,16 @@ cudaError_t detect_contacts(pcc_ctx* ctx, double tol, int phase, size_t* added, 
   if ((e = ctx->bin_of.reserve(3 * n, 0, s))) return e;
   if ((e = ctx->ghost.reserve(n, 0, s))) return e;
   if ((e = ctx->bbox.reserve(8, 0, s))) return e;
-  static const int init[6] = {2147483647, 2147483647, 2147483647, -2147483647 - 1, -2147483647 - 1,
-                              -2147483647 - 1};
+  static const int init[7] = {2147483647, 2147483647, 2147483647, -2147483647 - 1, -2147483647 - 1,
+                              -2147483647 - 1, 0};
   int* pinned = reinterpret_cast<int*>(ctx->pinned_ll);
   cudaMemcpyAsync(ctx->bbox.p, init, sizeof init, cudaMemcpyHostToDevice, s);  // pageable: staged at once
   k_bin<<<grid_for(n), kBlock, 0, s>>>(ctx->cells.view(), n, ctx->params.linked_cell_size, ctx->params.ghost_mode,
                                         ctx->bin_of.p, ctx->bbox.p, ctx->ghost.p);
   ctx->launches++;
-  cudaMemcpyAsync(pinned, ctx->bbox.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(pinned, ctx->bbox.p, 7 * sizeof(int), cudaMemcpyDeviceToHost, s);
   if ((e = cudaStreamSynchronize(s))) return e;
+  ctx->planar = pinned[6] == 0;
   long long nx = (long long)pinned[3] - pinned[0] + 1, ny = (long long)pinned[4] - pinned[1] + 1,
             nz = (long long)pinned[5] - pinned[2] + 1;
   long long nbins = nx * ny * nz;

@@ -375,6 +375,248 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   }
 }
 
+// ---------------------------------------------------------------- planar form
+// For a planar colony the D row of a constraint has three non-zero entries per
+// side (n_x, n_y and the z torque arm) and U three per cell (u_x, u_y, w_z);
+// every other term of the general kernel is an exact zero, and a running sum
+// that starts at +0 is unchanged by adding a signed zero, so skipping them
+// gives bit-identical results.  Operands are packed so each gather is one
+// 32-byte sector:
+//   per incidence entry  inc  = (D_x, D_y, D_t, s) of that side,
+//   per constraint       st   = (gamma, g, gamma_old, 0), ping-pong per iteration,
+//                        ij, n = (n_x, n_y), t = (t_iz, t_jz), s = (s_i, s_j),
+//   per cell             cell = (M_lin, M_rot, len, ldot_prev), u = (u_x, u_y, w_z, dldot).
+struct PlanarArgs {
+  long long m, n;
+  const int2* ij;
+  const double2 *nn, *tt, *ss;
+  double* phi;    // Phi on entry, phi_next on exit
+  double* gamma;  // gamma_0 on entry, gamma_{k-1} on exit
+  double4* st[2];
+  const int *inc_off, *inc_ent;
+  const double4 *inc, *cell;
+  double4* u;
+  double *U, *F, *sig, *ldot, *imp;  // general-layout outputs on residual iterations
+  double dt, lambda, tau, tol;
+  long long max_it;
+  double* partials;
+  long long nchunks;
+  SolverScalars* sc;
+  DevStatus* st_err;
+};
+
+__device__ __forceinline__ void planar_cell_pass(const PlanarArgs& a, long long p, int mode, const double4* stp,
+                                                 double alpha, bool final) {
+  double f0 = 0.0, f1 = 0.0, f5 = 0.0, sg = 0.0;
+  const int b = a.inc_off[p], e = a.inc_off[p + 1];
+  for (int k = b; k < e; ++k) {
+    const long long c = a.inc_ent[k] >> 1;
+    const double4 d = a.inc[k];
+    const double4 s = ldcg(stp + c);
+    const double gc = mode == 0 ? s.z : project(s.x, s.y, alpha);
+    const double diff = sub(gc, s.z);
+    f0 = add(f0, mul(d.x, diff));
+    f1 = add(f1, mul(d.y, diff));
+    f5 = add(f5, mul(d.z, diff));
+    sg = add(sg, mul(d.w, gc));
+  }
+  const double4 cl = a.cell[p];
+  const double ux = add(add(0.0, mul(cl.x, f0)), 0.0);
+  const double uy = add(add(0.0, mul(cl.x, f1)), 0.0);
+  const double wz = add(add(0.0, mul(cl.y, f5)), 0.0);
+  const double im = exp(vscale(-a.lambda, sg));
+  const double ld = vscale(dvd(1.0, a.tau), mul(cl.z, im));
+  a.u[p] = make_double4(ux, uy, wz, sub(ld, cl.w));
+  if (final) {
+    double* U = a.U + 6 * p;
+    double* F = a.F + 6 * p;
+    U[0] = ux;
+    U[1] = uy;
+    U[2] = 0.0;
+    U[3] = 0.0;
+    U[4] = 0.0;
+    U[5] = wz;
+    F[0] = f0;
+    F[1] = f1;
+    F[2] = 0.0;
+    F[3] = 0.0;
+    F[4] = 0.0;
+    F[5] = f5;
+    a.sig[p] = sg;
+    a.ldot[p] = ld;
+    a.imp[p] = im;
+  }
+}
+
+__device__ __forceinline__ double planar_grad(const PlanarArgs& a, long long c) {
+  const int2 ij = a.ij[c];
+  const double2 n = a.nn[c], t = a.tt[c], s = a.ss[c];
+  const double4 ui = ldcg(a.u + ij.x), uj = ldcg(a.u + ij.y);
+  double pd = 0.0;  // gi < gj: the i block comes first in column order
+  pd = add(pd, mul(n.x, ui.x));
+  pd = add(pd, mul(n.y, ui.y));
+  pd = add(pd, mul(t.x, ui.z));
+  pd = add(pd, mul(-n.x, uj.x));
+  pd = add(pd, mul(-n.y, uj.y));
+  pd = add(pd, mul(t.y, uj.z));
+  double gr = 0.0;
+  gr = add(gr, mul(s.x, ui.w));
+  gr = add(gr, mul(s.y, uj.w));
+  return add(a.phi[c], add(mul(a.dt, pd), mul(-a.dt, gr)));
+}
+
+__global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs a) {
+  __shared__ double sm[4 * kBlock];
+  const unsigned nb = gridDim.x;
+  const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
+  const long long stride = (long long)nb * kBlock;
+  SolverScalars* sc = a.sc;
+
+  for (long long p = tid; p < a.n; p += stride) planar_cell_pass(a, p, 0, a.st[0], 0.0, false);
+  if (!barrier(sc, nb, a.st_err)) return;
+  for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
+    double v[4] = {0, 0, 0, 0};
+    for (int k = 0; k < kPerThread; ++k) {
+      long long c = ch * kChunk + k * kBlock + threadIdx.x;
+      if (c >= a.m) break;
+      const double g = planar_grad(a, c);
+      const double gm = a.st[0][c].x;
+      a.st[0][c].y = g;
+      double r = proj_grad_abs(g, gm);
+      v[3] = v[3] < r ? r : v[3];
+    }
+    block_reduce4(v, sm);
+    if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
+  }
+  auto reduce_init = [&]() {
+    double v[4] = {0, 0, 0, 0};
+    for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
+      double r = ldcg(a.partials + 4 * ch + 3);
+      v[3] = v[3] < r ? r : v[3];
+    }
+    block_reduce4(v, sm);
+    if (threadIdx.x == 0) {
+      sc->res0 = v[3];
+      sc->residual = v[3];
+      sc->alpha = 1.0 / v[3];
+      sc->converged = 0;
+    }
+  };
+  if (!barrier_reduce(sc, nb, a.st_err, reduce_init)) return;
+
+  int p = 0;
+  long long it = 1;
+  while (it < a.max_it) {
+    const double alpha = *(volatile double*)&sc->alpha;
+    const bool check = (it % 10) == 0;
+    const double4* sp = a.st[p];
+    double4* so = a.st[1 - p];
+    for (long long q = tid; q < a.n; q += stride) planar_cell_pass(a, q, 1, sp, alpha, check);
+    if (!barrier(sc, nb, a.st_err)) return;
+    for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
+      double v[4] = {0, 0, 0, 0};
+      for (int k = 0; k < kPerThread; ++k) {
+        long long c = ch * kChunk + k * kBlock + threadIdx.x;
+        if (c >= a.m) break;
+        const double4 s = ldcg(sp + c);
+        const double gam = project(s.x, s.y, alpha);
+        const double g = planar_grad(a, c);
+        so[c] = make_double4(gam, g, s.z, 0.0);
+        const double dgm = sub(gam, s.x), dg = sub(g, s.y);
+        v[0] = add(v[0], mul(dgm, dgm));
+        v[1] = add(v[1], mul(dgm, dg));
+        v[2] = add(v[2], mul(dg, dg));
+        if (check) {
+          double r = proj_grad_abs(g, gam);
+          v[3] = v[3] < r ? r : v[3];
+        }
+      }
+      block_reduce4(v, sm);
+      if (threadIdx.x == 0) {
+        a.partials[4 * ch + 0] = v[0];
+        a.partials[4 * ch + 1] = v[1];
+        a.partials[4 * ch + 2] = v[2];
+        a.partials[4 * ch + 3] = v[3];
+      }
+    }
+    auto reduce_iter = [&]() {
+      double v[4] = {0, 0, 0, 0};
+      for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
+        v[0] = add(v[0], ldcg(a.partials + 4 * ch + 0));
+        v[1] = add(v[1], ldcg(a.partials + 4 * ch + 1));
+        v[2] = add(v[2], ldcg(a.partials + 4 * ch + 2));
+        double r = ldcg(a.partials + 4 * ch + 3);
+        v[3] = v[3] < r ? r : v[3];
+      }
+      block_reduce4(v, sm);
+      if (threadIdx.x == 0) {
+        int conv = 0;
+        if (check) {
+          sc->residual = v[3];
+          if (v[3] <= a.tol) conv = 1;
+        }
+        if (!conv) {
+          double num, den;
+          if (it % 2 == 0) {
+            num = v[0];
+            den = v[1];
+          } else {
+            den = v[2];
+            num = v[1];
+          }
+          if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
+          sc->alpha = dvd(num, den);
+        }
+        sc->converged = conv;
+        sc->iterations = it;
+      }
+    };
+    if (!barrier_reduce(sc, nb, a.st_err, reduce_iter)) return;
+    if (*(volatile int*)&sc->converged) break;
+    p = 1 - p;
+    ++it;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->iterations = it;
+  if (!*(volatile int*)&sc->converged) return;
+  for (long long c = tid; c < a.m; c += stride) {
+    a.gamma[c] = ldcg(a.st[p] + c).x;
+    a.phi[c] = ldcg(a.st[1 - p] + c).y;
+  }
+}
+
+// Packs the planar operands of one ReLCP phase.
+__global__ void k_pack_planar_cons(ConsView cs, long long m, int2* __restrict__ ij, double2* __restrict__ nn,
+                                   double2* __restrict__ tt, double2* __restrict__ ss, double4* __restrict__ st) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m) return;
+  ij[c] = make_int2(cs.gi[c], cs.gj[c]);
+  nn[c] = make_double2(cs.nx[c], cs.ny[c]);
+  tt[c] = make_double2(cs.tiz[c], cs.tjz[c]);
+  ss[c] = make_double2(cs.si[c], cs.sj[c]);
+  const double g = cs.gamma[c];
+  st[c] = make_double4(g, 0.0, g, 0.0);
+}
+
+__global__ void k_pack_planar_inc(ConsView cs, const int* __restrict__ inc_ent, long long ne,
+                                  double4* __restrict__ inc) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  const int ent = inc_ent[k];
+  const long long c = ent >> 1;
+  if ((ent & 1) == 0)
+    inc[k] = make_double4(cs.nx[c], cs.ny[c], cs.tiz[c], cs.si[c]);
+  else
+    inc[k] = make_double4(-cs.nx[c], -cs.ny[c], cs.tjz[c], cs.sj[c]);
+}
+
+__global__ void k_pack_planar_cells(const double* __restrict__ Ml, const double* __restrict__ Mr,
+                                    const double* __restrict__ len, const double* __restrict__ ldot_prev, long long n,
+                                    double4* __restrict__ cell) {
+  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  cell[p] = make_double4(Ml[p], Mr[p], len[p], ldot_prev[p]);
+}
+
 // Cell update after a solve: dC = G U (Physics.cpp:220-265), Euler step and
 // quaternion normalisation (simulation/Particle.cpp:37-57, 110-120), force,
 // velocity and growth parameters (ParticleManager.cpp:29-130).
@@ -616,18 +858,76 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   a.sc = ctx->scal.p;
   a.st = ctx->status;
 
-  if (ctx->coop_blocks == 0) {
+  const bool planar = ctx->planar && ctx->params.solver_variant != PCC_SOLVER_GENERAL;
+  PlanarArgs pa;
+  if (planar) {
+    const size_t ne = 2 * m;
+    if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_n.reserve(mm, 0, s)) || (e = ctx->p_t.reserve(mm, 0, s)) ||
+        (e = ctx->p_s.reserve(mm, 0, s)) || (e = ctx->p_st0.reserve(mm, 0, s)) || (e = ctx->p_st1.reserve(mm, 0, s)) ||
+        (e = ctx->p_inc.reserve(ne + 1, 0, s)) || (e = ctx->p_cell.reserve(nn, 0, s)) ||
+        (e = ctx->p_u.reserve(nn, 0, s)))
+      return e;
+    if (m) {
+      k_pack_planar_cons<<<grid_for((long long)m), kBlock, 0, s>>>(cv, (long long)m, ctx->p_ij.p, ctx->p_n.p,
+                                                                   ctx->p_t.p, ctx->p_s.p, ctx->p_st0.p);
+      k_pack_planar_inc<<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne, ctx->p_inc.p);
+      ctx->launches += 2;
+    }
+    if (n) {
+      k_pack_planar_cells<<<grid_for((long long)n), kBlock, 0, s>>>(ctx->Mlin.p, ctx->Mrot.p, ctx->cells.len.p,
+                                                                    ctx->cells.ldot.p, (long long)n, ctx->p_cell.p);
+      ctx->launches++;
+    }
+    pa.m = (long long)m;
+    pa.n = (long long)n;
+    pa.ij = ctx->p_ij.p;
+    pa.nn = ctx->p_n.p;
+    pa.tt = ctx->p_t.p;
+    pa.ss = ctx->p_s.p;
+    pa.phi = cv.sd;
+    pa.gamma = cv.gamma;
+    pa.st[0] = ctx->p_st0.p;
+    pa.st[1] = ctx->p_st1.p;
+    pa.inc_off = ctx->inc_off.p;
+    pa.inc_ent = ctx->inc_ent.p;
+    pa.inc = ctx->p_inc.p;
+    pa.cell = ctx->p_cell.p;
+    pa.u = ctx->p_u.p;
+    pa.U = ctx->U.p;
+    pa.F = ctx->F.p;
+    pa.sig = ctx->sig.p;
+    pa.ldot = ctx->ldot_new.p;
+    pa.imp = ctx->imp_new.p;
+    pa.dt = dt;
+    pa.lambda = ctx->params.lambda;
+    pa.tau = ctx->params.tau;
+    pa.tol = ctx->params.tolerance;
+    pa.max_it = ctx->params.max_bbpgd_iterations;
+    pa.partials = ctx->partials.p;
+    pa.nchunks = nchunks;
+    pa.sc = ctx->scal.p;
+    pa.st_err = ctx->status;
+  }
+  int& coop = planar ? ctx->coop_blocks_planar : ctx->coop_blocks;
+  if (coop == 0) {
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bbpgd, kBlock, 0))) return e;
-    ctx->coop_blocks = per_sm * ctx->num_sms;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, planar ? (const void*)k_bbpgd_planar
+                                                                           : (const void*)k_bbpgd,
+                                                           kBlock, 0)))
+      return e;
+    coop = per_sm * ctx->num_sms;
   }
   long long want = (long long)grid_for((long long)n);
   if (nchunks > want) want = nchunks;
-  if (want > ctx->coop_blocks) want = ctx->coop_blocks;
+  if (want > coop) want = coop;
   if (want < 1) want = 1;
   void* args[] = {&a};
+  void* pargs[] = {&pa};
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], s);
-  e = cudaLaunchCooperativeKernel((void*)k_bbpgd, dim3((unsigned)want), dim3(kBlock), args, 0, s);
+  if (planar)
+    e = cudaLaunchCooperativeKernel((void*)k_bbpgd_planar, dim3((unsigned)want), dim3(kBlock), pargs, 0, s);
+  else
+    e = cudaLaunchCooperativeKernel((void*)k_bbpgd, dim3((unsigned)want), dim3(kBlock), args, 0, s);
   ctx->launches++;
   if (e) return e;
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);

@@ -160,6 +160,50 @@ def test_solve_is_deterministic():
     assert max(d.values()) == 0.0, d
 
 
+@pytest.mark.parametrize("name", ["hard_r10_seed3", "hard_tight_r10_seed3"])
+def test_planar_solver_bit_identical_to_general(name):
+    """On a planar colony the packed 2D BBPGD kernel skips only exact zeros."""
+    fx = load_fixture(name)
+    out = []
+    for variant in (abi.SOLVER_AUTO, abi.SOLVER_GENERAL):
+        g = Colony(params_of(fx, solver_variant=variant))
+        g.set_cells(sub(fx, "cells_"))
+        st = g.solve(params_of(fx).dt, 0)
+        out.append((st, g.get_cells(), g.constraints()))
+    assert out[0][0] == out[1][0]
+    for k in ("x", "y", "z", "q0", "q1", "q2", "q3", "length", "ldot", "stress", "impedance", "force", "velocity"):
+        np.testing.assert_array_equal(out[0][1][k], out[1][1][k], err_msg=k)
+    for k in ("gamma", "sd"):
+        np.testing.assert_array_equal(out[0][2][k], out[1][2][k], err_msg=k)
+
+
+def test_non_planar_colony_matches_oracle():
+    """Cells tilted out of the plane take the general 3D path."""
+    fx = load_fixture("hard_r5_seed0_noghost")
+    cells = sub(fx, "cells_")
+    rng = np.random.default_rng(0)
+    n = len(cells["x"])
+    cells["z"] = rng.uniform(-0.05, 0.05, n)
+    tilt = rng.uniform(-0.05, 0.05, n)
+    q = np.stack([cells["q0"], np.sin(tilt / 2) * cells["q0"], np.zeros(n), cells["q3"]], 1)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    cells["q0"], cells["q1"], cells["q2"], cells["q3"] = q.T
+    p = params_of(fx)
+    g, o = Colony(p), OracleColony(p)
+    g.set_cells(cells)
+    o.set_cells(cells)
+    a, b = normalized_contacts(g.detect(0.25)), normalized_contacts(o.detect(0.25))
+    for k in b:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    g.set_cells(cells)
+    o.set_cells(cells)
+    sg, so = g.solve(p.dt, 0), o.solve(p.dt, 0)
+    assert sg["relcp_iterations"] == so["relcp_iterations"]
+    d = cells_max_diff(g.get_cells(), o.get_cells())
+    assert max(d.values()) < 1e-9, d
+    assert np.max(np.abs(g.get_cells()["q1"])) > 0
+
+
 def test_bbpgd_nonconvergence_raises_reference_message():
     fx = load_fixture("hard_r10_seed3")
     g = Colony(params_of(fx, max_bbpgd_iterations=5))
