@@ -200,6 +200,27 @@ pcc_status pcc_bbpgd_frozen(pcc_ctx* ctx, double dt, int repeats, long long* ite
                             float* ms_per_solve);
 pcc_status pcc_soft_forces_frozen(pcc_ctx* ctx, int repeats, float* ms_per_assembly);
 
+/* Soft-model force assembly that allocates no device memory.  It has no
+ * counterpart in the reference: it exists for hosts that must not let this
+ * library allocate -- a host that accounts its HBM through its own fixed pool
+ * (such as a serving loop admitting colonies against a byte budget), or a
+ * stepping loop sharing the GPU with other colonies' streams, where
+ * cudaFree's device-wide wait would stall them.  Every pointer is a device
+ * pointer the caller owns: contacts in the pcc_contacts layout (normal, r_i,
+ * r_j hold 3 values per contact) and the cell diameters are inputs; force
+ * (6 per cell: force, torque) and stress (1 per cell) are outputs, equal to
+ * the force assembly of pcc_soft_forces_frozen / solveSoftPotential
+ * (Soft.cpp:46-83).  Limit: 65536 cells and 393216 contacts per call
+ * (PCC_ERR_CAPACITY beyond, before any GPU work).  Intermediates live in one
+ * fixed 6.75 MiB device array that every call on a GPU shares, so calls must
+ * not overlap on one device; the first call on a device looks the array up
+ * and should come before any stream capture.  stream is a cudaStream_t
+ * (NULL: the default stream). */
+pcc_status pcc_soft_forces_noalloc(const int* gid_i, const int* gid_j, const double* sd, const double* normal,
+                                   const double* r_i, const double* r_j, const double* stress_i,
+                                   const double* stress_j, size_t m, const double* diameter, size_t n, double kcc,
+                                   double* force, double* stress, void* stream);
+
 /* The CUDA stream all work of the context is queued on (a cudaStream_t). */
 void* pcc_get_stream(const pcc_ctx* ctx);
 
