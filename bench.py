@@ -360,6 +360,66 @@ def run_frozen(args):
                       "frac_of_hbm": algo / (ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"]}), flush=True)
 
 
+def colony_jobs(n: int, rng, r_min: float, r_max: float, hard_frac: float, arrivals=None) -> list[dict]:
+    """Colony jobs as in the batch sweep / serving configs: sequential seeds,
+    growth rate g ~ U[0.5, 1.5] (tau = 1/g), R_end log-uniform in [r_min, r_max],
+    hard jobs with CFL-adaptive dt capped at 1e-3, soft jobs at dt = 3e-5 with
+    the Hertz constant of E = 1e3, R_eff = 0.125."""
+    jobs = []
+    for k in range(n):
+        hard = rng.random() < hard_frac
+        g = rng.uniform(0.5, 1.5)
+        r_end = float(np.exp(rng.uniform(np.log(r_min), np.log(r_max))))
+        if hard:
+            p = abi.default_params(mode=abi.MODE_HARD, seed=k, tau=1.0 / g, dt=1e-3, fixed_dt=0, dt_cap=1e-3)
+        else:
+            p = abi.default_params(mode=abi.MODE_SOFT, seed=k, tau=1.0 / g, dt=3e-5, fixed_dt=1,
+                                   kcc=1333.3333333333333)
+        jobs.append({"params": p, "end_radius": r_end, "arrival_s": 0.0 if arrivals is None else arrivals[k],
+                     "hard": hard})
+    return jobs
+
+
+def run_jobs(args):
+    """Batch sweep (--jobs N, all arrive at once) or serving (--rate R jobs/s,
+    Poisson arrivals for --serve-seconds): continuous batching with --slots
+    colonies in flight, against a sample of the same jobs one at a time."""
+    from pcc_b200 import build, device
+    build.build()
+    rng = np.random.default_rng(args.job_seed)
+    if args.rate > 0:
+        t, arr = 0.0, []
+        while True:
+            t += rng.exponential(1.0 / args.rate)
+            if t > args.serve_seconds:
+                break
+            arr.append(t)
+        jobs = colony_jobs(len(arr), rng, args.r_min, args.r_max, args.hard_frac, arr)
+    else:
+        jobs = colony_jobs(args.jobs, rng, args.r_min, args.r_max, args.hard_frac)
+    res, wall = device.serve(jobs, slots=args.slots, hbm_budget_bytes=args.hbm_budget)
+    lat = np.array([r["finish_s"] - r["arrival_s"] for r in res])
+    cells = sum(r["cell_steps"] for r in res)
+    sample = [dict(j, arrival_s=0.0) for j in jobs[: args.baseline_jobs]]
+    res1, wall1 = device.serve(sample, slots=1, hbm_budget_bytes=args.hbm_budget)
+    same = all(a["checksum"] == b["checksum"] and a["steps"] == b["steps"] for a, b in zip(res1, res))
+    seq_rate = sum(r["cell_steps"] for r in res1) / wall1
+    line = {
+        "metric": METRIC, "mode": "serve" if args.rate > 0 else "batch",
+        "jobs": len(jobs), "hard_jobs": sum(j["hard"] for j in jobs), "slots": args.slots,
+        "offered_jobs_per_s": args.rate if args.rate > 0 else None,
+        "colonies_per_s": len(jobs) / wall, "cell_steps_per_s": cells / wall, "wall_s": wall,
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max())},
+        "one_at_a_time": {"jobs": len(sample), "cell_steps_per_s": seq_rate, "wall_s": wall1},
+        "speedup_vs_one_at_a_time": (cells / wall) / seq_rate,
+        "results_identical_alone_and_in_mix": same,
+        "config": {"r_end": [args.r_min, args.r_max], "growth_rate": [0.5, 1.5], "hard_fraction": args.hard_frac,
+                   "hbm_budget_bytes": args.hbm_budget, "tolerance": 1e-3, "dtype": "f64"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,8 +430,20 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--verbose", action="store_true", help="per-step solver statistics on stderr")
     ap.add_argument("--frozen", action="store_true", help="BBPGD microbench on a frozen constraint set")
+    ap.add_argument("--jobs", type=int, default=0, help="batch sweep of N colonies (continuous batching)")
+    ap.add_argument("--rate", type=float, default=0.0, help="serving: Poisson arrivals per second")
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--slots", type=int, default=32)
+    ap.add_argument("--r-min", type=float, default=10.0)
+    ap.add_argument("--r-max", type=float, default=20.0)
+    ap.add_argument("--hard-frac", type=float, default=0.8)
+    ap.add_argument("--hbm-budget", type=float, default=150e9)
+    ap.add_argument("--baseline-jobs", type=int, default=8)
+    ap.add_argument("--job-seed", type=int, default=0)
     args = ap.parse_args()
-    if args.frozen:
+    if args.jobs > 0 or args.rate > 0:
+        run_jobs(args)
+    elif args.frozen:
         run_frozen(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -112,6 +112,7 @@ typedef struct pcc_cells {
   double *ldot, *impedance, *stress;  /* optional */
   int *age;                           /* optional */
   double *force, *velocity;           /* optional, 6 per cell */
+  int *num_constraints;               /* optional, download only: contacts counted during the last solve */
 } pcc_cells;
 
 /* Host SoA view of constraints (Constraint, dynamics/Constraint.h:6-49). */
@@ -152,6 +153,8 @@ typedef struct pcc_profile {
   double solve_ms;              /* whole pcc_solve calls */
   long long solves;
   double cell_solves;           /* sum of cell counts over solves */
+  long long detect_full_passes; /* detections that rebinned the colony (counted with profiling off too) */
+  long long detect_list_passes; /* later ReLCP phases served from the candidate lists */
 } pcc_profile;
 
 typedef struct pcc_ctx pcc_ctx;
@@ -220,6 +223,38 @@ pcc_status pcc_soft_forces_noalloc(const int* gid_i, const int* gid_j, const dou
                                    const double* r_i, const double* r_j, const double* stress_i,
                                    const double* stress_j, size_t m, const double* diameter, size_t n, double kcc,
                                    double* force, double* stress, void* stream);
+
+/* One colony job of a batch sweep or a serving stream: grow one colony from a
+ * single cell (orientation theta ~ U[0, pi) drawn from params.seed) until its
+ * radius reaches end_radius. */
+typedef struct pcc_job {
+  pcc_params params;   /* per job: mode, seed, tau (= 1 / growth rate), tolerances, ... */
+  double end_radius;
+  double arrival_s;    /* arrival time after the start of pcc_serve (0: immediately) */
+  long long max_steps; /* 0: no cap */
+} pcc_job;
+
+typedef struct pcc_job_result {
+  int status;                  /* pcc_status of the job */
+  long long steps;
+  long long cells;             /* final cell count */
+  double cell_steps;           /* sum over steps of the cell count */
+  long long bbpgd_iterations;
+  double arrival_s, start_s, finish_s;  /* seconds after the start of pcc_serve */
+  double footprint_bytes;      /* projected device footprint used for admission */
+  double checksum;             /* sum over final cells of x+y+z+q0+q1+q2+q3+length */
+} pcc_job_result;
+
+/* Continuous batching of independent colonies (no counterpart in the
+ * reference, which runs one colony per MPI job): runs the jobs with at most
+ * `slots` in flight, each on its own context, CUDA stream and host thread so
+ * their kernels overlap on the device.  A job is admitted, in arrival order,
+ * once it has arrived, a slot is free and its projected device footprint at
+ * end_radius fits in hbm_budget_bytes beside the jobs in flight; a finishing
+ * job frees its slot and budget.  Results are bit-identical alone and in any
+ * mix.  Returns the first failing job's status (all results are filled). */
+pcc_status pcc_serve(const pcc_job* jobs, size_t n_jobs, int slots, double hbm_budget_bytes, int device,
+                     pcc_job_result* results, double* wall_s);
 
 /* The CUDA stream all work of the context is queued on (a cudaStream_t). */
 void* pcc_get_stream(const pcc_ctx* ctx);

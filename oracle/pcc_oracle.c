@@ -32,6 +32,7 @@ typedef struct {
   double q[4];
   double len, l0, diam, ldot, imp, stress;
   int age;
+  int nc; /* Particle::num_constraints_ */
   double force[6], vel[6];
 } cell_t;
 
@@ -337,6 +338,11 @@ static cons_t* detect(pcco_colony* col, double tol, int phase, size_t* nout) {
             if (b <= a) continue;
             cons_t cs;
             if (!try_constraint(&col->cells[a], &col->cells[b], (int)a, (int)b, tol, phase, &cs)) continue;
+            /* incrementNumConstraints (CollisionDetector.cpp:243-244) runs for every
+             * passing candidate, including the variants with ghost copies; counts
+             * of a cell that has a self-ghost go to the ghost copy and are lost. */
+            if (!ghost[a]) col->cells[a].nc += 1 + ghost[b];
+            if (!ghost[b]) col->cells[b].nc += 1 + ghost[a];
             int copies = 1 + (ghost[b] ? 1 : 0);
             for (int k2 = 0; k2 < copies; ++k2) {
               if (cnt == cap) {
@@ -1015,6 +1021,7 @@ int pcco_get_cells(pcco_colony* c, pcc_cells* o, size_t cap, size_t* n) {
     if (o->impedance) o->impedance[i] = x->imp;
     if (o->stress) o->stress[i] = x->stress;
     if (o->age) o->age[i] = x->age;
+    if (o->num_constraints) o->num_constraints[i] = x->nc;
     if (o->force) memcpy(o->force + 6 * i, x->force, sizeof x->force);
     if (o->velocity) memcpy(o->velocity + 6 * i, x->vel, sizeof x->vel);
   }
@@ -1027,7 +1034,10 @@ int pcco_solve(pcco_colony* c, double dt, int iter, pcc_step_stats* st) {
     snprintf(c->err, sizeof c->err, "temperature > 0 (Brownian kicks) is not restated");
     return PCC_ERR_INVALID;
   }
-  for (size_t i = 0; i < c->n; ++i) c->cells[i].ldot = 0.0; /* Particle::reset (Particle.h:146-149) */
+  for (size_t i = 0; i < c->n; ++i) { /* Particle::reset (Particle.h:146-149) */
+    c->cells[i].ldot = 0.0;
+    c->cells[i].nc = 0;
+  }
   int rc = c->p.mode == PCC_MODE_SOFT ? solve_soft(c, dt, st) : solve_hard(c, dt, st);
   if (st) st->dt_used = dt;
   return rc;

@@ -199,6 +199,7 @@ int pcc_ref_get_cells(void* h, pcc_cells* out, size_t cap, size_t* n) {
     if (out->impedance) out->impedance[i] = p.getImpedance();
     if (out->stress) out->stress[i] = p.getStress();
     if (out->age) out->age[i] = d.age;
+    if (out->num_constraints) out->num_constraints[i] = p.getNumConstraints();
     if (out->force) {
       for (int k = 0; k < 3; ++k) out->force[6 * i + k] = p.getForce()[k];
       for (int k = 0; k < 3; ++k) out->force[6 * i + 3 + k] = p.getTorque()[k];

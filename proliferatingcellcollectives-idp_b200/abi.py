@@ -67,7 +67,8 @@ class Params(C.Structure):
 class Cells(C.Structure):
     _fields_ = [(n, _dp) for n in ("x", "y", "z", "q0", "q1", "q2", "q3", "length", "l0", "diameter",
                                    "ldot", "impedance", "stress")] + [("age", _ip), ("force", _dp),
-                                                                      ("velocity", _dp)]
+                                                                      ("velocity", _dp),
+                                                                      ("num_constraints", _ip)]
 
 
 class Contacts(C.Structure):
@@ -104,6 +105,31 @@ class Profile(C.Structure):
         ("solve_ms", C.c_double),
         ("solves", C.c_longlong),
         ("cell_solves", C.c_double),
+        ("detect_full_passes", C.c_longlong),
+        ("detect_list_passes", C.c_longlong),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Job(C.Structure):
+    _fields_ = [("params", Params), ("end_radius", C.c_double), ("arrival_s", C.c_double),
+                ("max_steps", C.c_longlong)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [
+        ("status", C.c_int),
+        ("steps", C.c_longlong),
+        ("cells", C.c_longlong),
+        ("cell_steps", C.c_double),
+        ("bbpgd_iterations", C.c_longlong),
+        ("arrival_s", C.c_double),
+        ("start_s", C.c_double),
+        ("finish_s", C.c_double),
+        ("footprint_bytes", C.c_double),
+        ("checksum", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -157,10 +183,12 @@ class CellArrays:
         self.arrays["age"] = np.zeros(max(self.cap, 1), np.int32)
         self.arrays["force"] = np.zeros(6 * max(self.cap, 1), np.float64)
         self.arrays["velocity"] = np.zeros(6 * max(self.cap, 1), np.float64)
+        self.arrays["num_constraints"] = np.zeros(max(self.cap, 1), np.int32)
         self.struct = Cells()
         for f in CELL_FIELDS + ("force", "velocity"):
             setattr(self.struct, f, self.arrays[f].ctypes.data_as(_dp))
         self.struct.age = self.arrays["age"].ctypes.data_as(_ip)
+        self.struct.num_constraints = self.arrays["num_constraints"].ctypes.data_as(_ip)
 
     @classmethod
     def from_dict(cls, cells: dict) -> "CellArrays":
@@ -173,7 +201,7 @@ class CellArrays:
         return ca
 
     def to_dict(self, n: int) -> dict:
-        out = {f: self.arrays[f][:n].copy() for f in CELL_FIELDS + ("age",)}
+        out = {f: self.arrays[f][:n].copy() for f in CELL_FIELDS + ("age", "num_constraints")}
         out["force"] = self.arrays["force"][: 6 * n].reshape(n, 6).copy()
         out["velocity"] = self.arrays["velocity"][: 6 * n].reshape(n, 6).copy()
         return out

@@ -24,12 +24,13 @@ cudaError_t CellBufs::reserve(size_t n, size_t keep, cudaStream_t s) {
   if ((e = force.reserve(6 * (n + 1), 6 * keep, s))) return e;
   if ((e = vel.reserve(6 * (n + 1), 6 * keep, s))) return e;
   if ((e = age.reserve(n + 1, keep, s))) return e;
+  if ((e = ncons.reserve(n + 1, keep, s))) return e;
   return cudaSuccess;
 }
 
 CellsView CellBufs::view() {
   return CellsView{x.p, y.p, z.p, q0.p, q1.p, q2.p, q3.p, len.p, l0.p, diam.p, ldot.p, imp.p, stress.p, age.p,
-                   force.p, vel.p};
+                   force.p, vel.p, ncons.p};
 }
 
 template <typename T>
@@ -59,6 +60,7 @@ void CellBufs::swap(CellBufs& o) {
   swap_buf(force, o.force);
   swap_buf(vel, o.vel);
   swap_buf(age, o.age);
+  swap_buf(ncons, o.ncons);
 }
 
 cudaError_t ConsBufs::reserve(size_t n, size_t keep, cudaStream_t s) {
@@ -143,7 +145,7 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
     if (before) CU(max_overlap(ctx, 0, before, &ov_old), "max_overlap");
     size_t added = 0;
     if (ctx->profiling) cudaEventRecord(ctx->ev[2], ctx->stream);
-    CU(detect_contacts(ctx, phase == 0 ? .25 : tol, phase, &added, &ov_new), "detect");
+    CU(detect_contacts(ctx, phase == 0 ? .25 : tol, phase, phase > 0, &added, &ov_new), "detect");
     max_ov = ov_old < ov_new ? ov_new : ov_old;
     if (max_ov <= tol && phase > 0) {
       profile_detect(ctx);
@@ -185,7 +187,7 @@ pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
   size_t added = 0;
   double max_ov = 0.0;
   if (ctx->profiling) cudaEventRecord(ctx->ev[2], ctx->stream);
-  CU(detect_contacts(ctx, 0.0, 0, &added, &max_ov), "detect");
+  CU(detect_contacts(ctx, 0.0, 0, false, &added, &max_ov), "detect");
   CU(build_incidence(ctx), "incidence");
   profile_detect(ctx);
   CU(soft_forces_and_move(ctx, dt), "soft");
@@ -353,6 +355,7 @@ pcc_status pcc_upload_cells(pcc_ctx* ctx, const pcc_cells* c, size_t n) {
     cudaMemcpyAsync(v.age, ones.data(), n * sizeof(int), cudaMemcpyHostToDevice, s);
     CU(cudaStreamSynchronize(s), "upload");
   }
+  if (n) cudaMemsetAsync(v.ncons, 0, n * sizeof(int), s);
   ctx->n = n;
   ctx->ncons = 0;
   CU(cudaStreamSynchronize(s), "upload");
@@ -393,6 +396,7 @@ pcc_status pcc_download_cells(pcc_ctx* ctx, pcc_cells* c, size_t cap, size_t* n)
   d2h(c->force, v.force, 6 * m);
   d2h(c->velocity, v.vel, 6 * m);
   if (c->age && m) cudaMemcpyAsync(c->age, v.age, m * sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (c->num_constraints && m) cudaMemcpyAsync(c->num_constraints, v.ncons, m * sizeof(int), cudaMemcpyDeviceToHost, s);
   CU(cudaStreamSynchronize(s), "download");
   return PCC_OK;
 }
@@ -404,6 +408,7 @@ pcc_status pcc_solve(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* out) {
   pcc_step_stats st;
   std::memset(&st, 0, sizeof st);
   if (ctx->profiling) cudaEventRecord(ctx->ev[4], ctx->stream);
+  if (ctx->n) CU(cudaMemsetAsync(ctx->cells.ncons.p, 0, ctx->n * sizeof(int), ctx->stream), "reset");  // Particle::reset
   pcc_status rc = ctx->params.mode == PCC_MODE_SOFT ? solve_soft(ctx, dt, &st) : solve_hard(ctx, dt, &st);
   st.dt_used = dt;
   if (ctx->profiling) {
@@ -475,7 +480,7 @@ pcc_status pcc_detect_contacts(pcc_ctx* ctx, double tol, int phase, pcc_contacts
   ctx->ncons = 0;
   size_t added = 0;
   double mo = 0;
-  CU(detect_contacts(ctx, tol, phase, &added, &mo), "detect");
+  CU(detect_contacts(ctx, tol, phase, false, &added, &mo), "detect");
   pcc_status rc = check_device(ctx, "detect");
   if (rc) return rc;
   *n = ctx->ncons;
@@ -503,7 +508,7 @@ pcc_status pcc_bbpgd_frozen(pcc_ctx* ctx, double dt, int repeats, long long* ite
   double mo = 0;
   CU(reset_ldot(ctx), "reset");
   CU(mobility(ctx), "mobility");
-  CU(detect_contacts(ctx, 0.25, 0, &added, &mo), "detect");
+  CU(detect_contacts(ctx, 0.25, 0, false, &added, &mo), "detect");
   CU(build_incidence(ctx), "incidence");
   const size_t m = ctx->ncons;
   DevBuf<double> sd0, g0;
@@ -517,7 +522,7 @@ pcc_status pcc_bbpgd_frozen(pcc_ctx* ctx, double dt, int repeats, long long* ite
   float total = 0;
   long long it = 0;
   double res = 0;
-  for (int r = 0; r < repeats; ++r) {
+  for (int r = 0; r <= repeats; ++r) {  // solve 0 is an untimed warm-up (buffers, occupancy query)
     cudaMemcpyAsync(ctx->cons.sd.p, sd0.p, m * sizeof(double), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(ctx->cons.gamma.p, g0.p, m * sizeof(double), cudaMemcpyDeviceToDevice, s);
     cudaEventRecord(a, s);
@@ -527,7 +532,7 @@ pcc_status pcc_bbpgd_frozen(pcc_ctx* ctx, double dt, int repeats, long long* ite
     cudaEventSynchronize(b);
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);
-    total += ms;
+    if (r > 0) total += ms;
     if (e) {
       cudaEventDestroy(a);
       cudaEventDestroy(b);
@@ -554,7 +559,7 @@ pcc_status pcc_soft_forces_frozen(pcc_ctx* ctx, int repeats, float* ms_per_assem
   ctx->ncons = 0;
   size_t added = 0;
   double mo = 0;
-  CU(detect_contacts(ctx, 0.0, 0, &added, &mo), "detect");
+  CU(detect_contacts(ctx, 0.0, 0, false, &added, &mo), "detect");
   CU(build_incidence(ctx), "incidence");
   cudaEvent_t a, b;
   cudaEventCreate(&a);

@@ -25,7 +25,11 @@ enum : unsigned {
 struct DevStatus {
   unsigned flags;
   int where;
-  unsigned long long max_bits;  // running max of a non-negative double (bit pattern)
+  unsigned long long max_bits;    // running max of a non-negative double (bit pattern)
+  unsigned list_flags;            // contact detection: candidate lists overflowed / stale
+  unsigned pad;
+  unsigned long long drift_bits;  // largest squared displacement since the lists were built
+  unsigned long long lmax_bits;   // longest cell
 };
 
 // Cell arrays (device pointers).
@@ -35,6 +39,7 @@ struct CellsView {
   int* age;
   double* force;  // 6 per cell
   double* vel;    // 6 per cell
+  int* ncons;     // contacts counted during the last solve (Particle::getNumConstraints)
 };
 
 // Constraint arrays (device pointers).  D row of constraint c

@@ -48,7 +48,7 @@ struct DevBuf {
 // All per-cell arrays (one set; the x-sort gathers into a second set and swaps).
 struct CellBufs {
   DevBuf<double> x, y, z, q0, q1, q2, q3, len, l0, diam, ldot, imp, stress, force, vel;
-  DevBuf<int> age;
+  DevBuf<int> age, ncons;
   cudaError_t reserve(size_t n, size_t keep, cudaStream_t s);
   CellsView view();
   void swap(CellBufs& o);
@@ -95,7 +95,13 @@ struct pcc_ctx {
   pcc::DevBuf<int> bin_of, bin_cnt, bin_off, bin_cursor, bin_cells, cand_cnt, cand_off;
   pcc::DevBuf<double> pk;  // packed per-cell geometry in bin order
   pcc::DevBuf<int> ghost;
-  pcc::DevBuf<int> bbox;   // [6] min/max bin coordinates
+  pcc::DevBuf<int> bbox;   // [6] min/max bin coordinates, [7] non-planar flag
+  // candidate partner lists of the last full neighbourhood pass (list-major)
+  pcc::DevBuf<int> plist, plist_n, slot_of;
+  pcc::DevBuf<double> xref;  // cell positions when the lists were built
+  bool list_valid = false;
+  size_t list_n = 0;
+  double list_tol = 0.0;
 
   // incidence CSR (cell -> constraint sides)
   pcc::DevBuf<int> inc_cnt, inc_off, inc_ent;

@@ -17,7 +17,11 @@ cudaError_t radix_sort_pairs(pcc_ctx* ctx, unsigned long long* keys, int* vals, 
 // ---- pcc_detect.cu
 // Appends the contacts within tol of the resident cells to the constraint set
 // (ctx->ncons grows by *added).  *max_overlap_new = max(-sd, 0) over them.
-cudaError_t detect_contacts(pcc_ctx* ctx, double tol, int phase, size_t* added, double* max_overlap_new);
+// reuse = true lets a later ReLCP phase of the same step re-test the
+// candidate lists of the previous full pass instead of rebinning; callers
+// pass it only when the cells changed by constraint motion alone since.
+cudaError_t detect_contacts(pcc_ctx* ctx, double tol, int phase, bool reuse, size_t* added,
+                            double* max_overlap_new);
 // Cell -> incident constraint sides, ascending constraint index, for ctx->ncons.
 cudaError_t build_incidence(pcc_ctx* ctx);
 

@@ -111,6 +111,7 @@ __global__ void k_divide(CellsView c, long long n, const int* __restrict__ flag,
   const int age = c.age[i] + 1;
   c.age[i] = age;
   c.age[j] = age;
+  c.ncons[j] = 0;
   c.ldot[j] = 0.0;
   c.imp[j] = 0.0;
   c.stress[j] = 0.0;
@@ -146,6 +147,7 @@ __global__ void k_gather_cells(CellsView src, CellsView dst, const int* __restri
   dst.imp[j] = src.imp[i];
   dst.stress[j] = src.stress[i];
   dst.age[j] = src.age[i];
+  dst.ncons[j] = src.ncons[i];
   for (int d = 0; d < 6; ++d) {
     dst.force[6 * j + d] = src.force[6 * (long long)i + d];
     dst.vel[6 * j + d] = src.vel[6 * (long long)i + d];

@@ -50,6 +50,8 @@ def load_library(path: str | os.PathLike | None = None):
     lib.pcc_set_profiling.argtypes = [VP, C.c_int]
     lib.pcc_reset_profile.argtypes = [VP]
     lib.pcc_get_profile.argtypes = [VP, P(abi.Profile)]
+    lib.pcc_serve.argtypes = [P(abi.Job), C.c_size_t, C.c_int, C.c_double, C.c_int, P(abi.JobResult),
+                              P(C.c_double)]
     lib.pcc_get_stream.restype = VP
     lib.pcc_get_stream.argtypes = [VP]
     lib.pcc_launch_count.restype = C.c_longlong
@@ -197,6 +199,28 @@ class Colony:
     @property
     def launches(self) -> int:
         return int(self.lib.pcc_launch_count(self.h))
+
+
+def serve(jobs: list[dict], slots: int, hbm_budget_bytes: float = 150e9, device: int = 0):
+    """Runs colony jobs with continuous batching (pcc_serve).  Each job is a
+    dict with 'params' (abi.Params), 'end_radius' and optional 'arrival_s',
+    'max_steps'.  Returns (list of result dicts, wall seconds); raises
+    PccError if a job failed."""
+    lib = load_library()
+    n = len(jobs)
+    arr = (abi.Job * max(n, 1))()
+    for i, j in enumerate(jobs):
+        arr[i].params = j["params"]
+        arr[i].end_radius = float(j["end_radius"])
+        arr[i].arrival_s = float(j.get("arrival_s", 0.0))
+        arr[i].max_steps = int(j.get("max_steps", 0))
+    res = (abi.JobResult * max(n, 1))()
+    wall = C.c_double(0)
+    rc = lib.pcc_serve(arr, n, int(slots), float(hbm_budget_bytes), device, res, C.byref(wall))
+    out = [res[i].as_dict() for i in range(n)]
+    if rc != 0:
+        raise PccError(rc, _REFERENCE_MESSAGES.get(rc, f"pcc_serve: {abi.STATUS_NAMES.get(rc, rc)}"))
+    return out, wall.value
 
 
 def division_length(seed: int, k: int, length: float) -> float:

@@ -220,3 +220,61 @@ def test_relcp_exhaustion_raises_reference_message():
     with pytest.raises(PccError, match="Maximum number of constraint iterations reached") as e:
         g.solve(1e-3, 0)
     assert e.value.status == abi.PCC_ERR_NOCONV_RELCP
+
+
+def _rows(c: dict) -> list:
+    """Constraint rows as a sorted multiset of (phase, smaller id, larger id)."""
+    a = np.minimum(c["gid_i"], c["gid_j"])
+    b = np.maximum(c["gid_i"], c["gid_j"])
+    return sorted(zip(np.asarray(c["phase"]).tolist(), a.tolist(), b.tolist()))
+
+
+def test_later_relcp_phases_reuse_candidate_lists():
+    """ReLCP phases after the first re-test the first phase's candidate lists
+    instead of rebinning; every phase's constraint rows and the per-cell
+    contact counts (Particle::num_constraints) are the reference's."""
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx)
+    g = Colony(p)
+    g.set_cells(sub(fx, "cells_"))
+    g.profiling(False)
+    st = g.solve(p.dt, 0)
+    want = fx["solve_stats"][0]
+    assert st["relcp_iterations"] == want["relcp_iterations"] == 4
+    pr = g.profile()
+    assert pr["detect_full_passes"] == 1 and pr["detect_list_passes"] == 4, pr
+    assert _rows(g.constraints()) == _rows(sub(fx, "solve_cons_"))
+    np.testing.assert_array_equal(g.get_cells()["num_constraints"], fx["solve_cells_num_constraints"])
+
+
+@pytest.mark.parametrize("over", [{"tolerance": 0.3}, {"linked_cell_size": 1.95}])
+def test_candidate_lists_fall_back_to_full_pass(over):
+    """When the displacement bound cannot prove the lists complete (a later
+    tolerance beyond the list reach; bins shorter than the longest cell plus
+    the reach) every phase rebins, and the result is the oracle's."""
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx, **over)
+    g, o = Colony(p), OracleColony(p)
+    g.set_cells(sub(fx, "cells_"))
+    o.set_cells(sub(fx, "cells_"))
+    g.profiling(False)
+    sg, so = g.solve(p.dt, 0), o.solve(p.dt, 0)
+    pr = g.profile()
+    assert pr["detect_list_passes"] == 0 and pr["detect_full_passes"] == sg["relcp_iterations"] + 1, pr
+    assert sg["relcp_iterations"] == so["relcp_iterations"]
+    assert _rows(g.constraints()) == _rows(o.constraints())
+    np.testing.assert_array_equal(g.get_cells()["num_constraints"], o.get_cells()["num_constraints"])
+    d = cells_max_diff(g.get_cells(), o.get_cells())
+    assert max(d.values()) < 1e-6, d
+
+
+@pytest.mark.parametrize("name", ["soft_on_hard_r10_seed3", "soft_r3_seed1", "hard_r5_seed0_noghost"])
+def test_num_constraints_match_reference(name):
+    """Particle::num_constraints after one call, including the counts a cell
+    with a self-ghost loses to its copy."""
+    fx = load_fixture(name)
+    p = params_of(fx)
+    g = Colony(p)
+    g.set_cells(sub(fx, "cells_"))
+    g.solve(p.dt, 0)
+    np.testing.assert_array_equal(g.get_cells()["num_constraints"], fx["solve_cells_num_constraints"])

@@ -49,7 +49,8 @@ def test_one_solve_bit_exact(name):
         assert st[k] == want[k], k
     got = o.get_cells()
     ref = sub(fx, "solve_cells_")
-    for k in ("x", "y", "z", "q0", "q1", "q2", "q3", "length", "ldot", "impedance", "stress", "force", "velocity"):
+    for k in ("x", "y", "z", "q0", "q1", "q2", "q3", "length", "ldot", "impedance", "stress", "force", "velocity",
+              "num_constraints"):
         np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
     gc = normalized_contacts(o.constraints())
     rc = normalized_contacts(sub(fx, "solve_cons_"))
