@@ -42,6 +42,9 @@ METRIC = "cell-steps/s to R_end; served colonies/s, p50/p99 vs plain GPU at same
 UNIT = "cell-steps/s"
 RADIUS = 260.0
 CPU_SAMPLE_RADIUS = 40.0  # bounded sample for the CPU legs (~5e3 cells)
+# algorithmic bytes of one BBPGD iteration per constraint and per cell (the
+# mixed-precision form halves the floating-point operand terms)
+ALGO_BYTES = {"fp64": (312.0, 288.0), "mixed": (192.0, 144.0)}
 
 
 def colony_params(**over) -> abi.Params:
@@ -60,10 +63,11 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
 
 
-def traffic_ratio() -> float | None:
-    """DRAM bytes / algorithmic bytes of the BBPGD kernel from the committed ncu
-    summary (profiles/k_bbpgd_*.md, line 'dram_to_algorithmic: <ratio>')."""
-    for f in sorted((ROOT / "profiles").glob("k_bbpgd_*.md")):
+def traffic_ratio(profile: str) -> float | None:
+    """DRAM bytes / algorithmic bytes of a BBPGD kernel from its committed ncu
+    summary (profiles/<profile>.md, line 'dram_to_algorithmic: <ratio>')."""
+    f = ROOT / "profiles" / f"{profile}.md"
+    if f.exists():
         m = re.search(r"dram_to_algorithmic:\s*([0-9.eE+-]+)", f.read_text())
         if m:
             return float(m.group(1))
@@ -225,12 +229,14 @@ def run_ours(args):
     import torch
     torch.cuda.init()
     cells = make_colony(args.radius, seed=rank)
-    p = colony_params(capacity_hint=int(len(cells["x"]) * 1.5))
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
+    p = colony_params(capacity_hint=int(len(cells["x"]) * 1.5), precision=prec)
     col = device.Colony(p, device=local)
     col.set_cells(cells)
     stream = torch.cuda.ExternalStream(col.stream, device=f"cuda:{local}")
     for _ in range(args.warmup):
         col.step()
+    errors = precision_errors(device, col, p, local) if rank == 0 and prec == abi.PRECISION_MIXED else None
     col.profiling(True)
     launches0 = col.launches
     barrier(world)
@@ -299,14 +305,17 @@ def run_ours(args):
     peaks = measured_peaks()
     bb_ms = prof["bbpgd_ms"]
     achieved = prof["bbpgd_algo_bytes"] / (bb_ms / 1e3) / 1e9 if bb_ms > 0 else 0.0
-    ratio = traffic_ratio()
+    mixed = prec == abi.PRECISION_MIXED
+    ratio = traffic_ratio("k_bbpgd_planar_mixed_frozen_r260" if mixed else "k_bbpgd_planar_frozen_r260")
     launches_bb = max(prof["bbpgd_launches"], 1)
     traffic = ratio * prof["bbpgd_algo_bytes"] / launches_bb if ratio else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"hard model colony step, FP64, synthetic dense colony R={args.radius:g}",
+        "vs_baseline": None, "dtype": "f64" if prec == abi.PRECISION_FP64 else "f32 operands / f64 accumulation",
+        "data": "synthetic",
+        "config": {"workload": f"hard model colony step, {'FP64' if prec == abi.PRECISION_FP64 else 'mixed precision'}"
+                               f", synthetic dense colony R={args.radius:g}",
                    "cells_per_rank": int(hist[0]["n_cells"]), "ghost_mode": "single_rank",
                    "tolerance": p.tolerance, "dt_start": 3e-4, "dt_cap": 1e-3,
                    "parallelism": f"replicas x{world}",
@@ -314,7 +323,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved,
                      "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
-                     "traffic": traffic, "kernel": "k_bbpgd (persistent BBPGD)",
+                     "traffic": traffic,
+                     "kernel": f"k_bbpgd_planar<{'float' if mixed else 'double'}> (persistent BBPGD)",
                      "peak_source": "fallback" if peaks.get("fallback") else "measured"},
         "bbpgd_iterations_per_s": prof["bbpgd_iterations"] / (ms / 1e3),
         "bbpgd_iterations_per_step": prof["bbpgd_iterations"] / max(args.steps, 1),
@@ -324,6 +334,8 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    if errors is not None:
+        line["mixed_vs_fp64"] = errors
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, kind, k, ncpu, el = cpu_rate(True)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
@@ -338,13 +350,63 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def packing_fraction(c: dict) -> float:
+    """Cell area (2D spherocylinders) over the area of the colony disk, whose
+    radius is the largest distance of a segment end from the origin."""
+    d, L = np.asarray(c["diameter"]), np.asarray(c["length"])
+    th = 2.0 * np.arctan2(np.asarray(c["q3"]), np.asarray(c["q0"]))
+    half = L / 2 - d / 2
+    x, y = np.asarray(c["x"]), np.asarray(c["y"])
+    ex, ey = half * np.cos(th), half * np.sin(th)
+    r = np.sqrt(np.maximum((x + ex) ** 2 + (y + ey) ** 2, (x - ex) ** 2 + (y - ey) ** 2))
+    area = np.sum(np.pi * d * d / 4 + d * (L - d))
+    return float(area / (np.pi * r.max() ** 2))
+
+
+def precision_errors(device, col, p, local) -> dict:
+    """One solver call from the same state with the FP64 and the mixed-precision
+    solver: errors of gamma (phase-0 rows, identical in both), cell forces and
+    positions, and the packing fraction, relative to FP64."""
+    snap = col.get_cells()
+    dt = col.dt
+    out = {}
+    for name, prec in (("fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
+        q = abi.Params.from_buffer_copy(p)
+        q.precision = prec
+        c = device.Colony(q, device=local)
+        c.set_cells(snap)
+        st = c.solve(dt, 0)
+        out[name] = (st, c.get_cells(), c.constraints())
+        c.close()
+    (s0, c0, k0), (s1, c1, k1) = out["fp64"], out["mixed"]
+    r0 = k0["phase"] == 0
+    r1 = k1["phase"] == 0
+    g0, g1 = k0["gamma"][r0], k1["gamma"][r1]
+    same_rows = bool(r0.sum() == r1.sum() and np.array_equal(k0["gid_i"][r0], k1["gid_i"][r1]))
+    f0, f1 = c0["force"], c1["force"]
+    return {
+        "state": f"after the warm-up steps ({len(snap['x'])} cells), one solver call each",
+        "gamma_phase0_max_abs": float(np.max(np.abs(g0 - g1))) if same_rows else None,
+        "gamma_phase0_rel": float(np.max(np.abs(g0 - g1)) / max(np.max(np.abs(g0)), 1e-300)) if same_rows else None,
+        "force_rel": float(np.max(np.abs(f0 - f1)) / max(np.max(np.abs(f0)), 1e-300)),
+        "position_max_abs": float(max(np.max(np.abs(c0[k] - c1[k])) for k in ("x", "y"))),
+        "packing_fraction": {"fp64": packing_fraction(c0), "mixed": packing_fraction(c1)},
+        "residual": {"fp64": s0["residual"], "mixed": s1["residual"]},
+        "max_overlap": {"fp64": s0["max_overlap"], "mixed": s1["max_overlap"]},
+        "bbpgd_iterations": {"fp64": s0["bbpgd_iterations"], "mixed": s1["bbpgd_iterations"]},
+        "relcp_iterations": {"fp64": s0["relcp_iterations"], "mixed": s1["relcp_iterations"]},
+        "tolerance": p.tolerance,
+    }
+
+
 def run_frozen(args):
     """BBPGD microbench on a frozen state: after W warm-up steps, detect the
     phase-0 contacts once and time `--steps` solves of that constraint set
     (the captured launch of the committed ncu summaries)."""
     from pcc_b200 import device
     cells = make_colony(args.radius, seed=0)
-    col = device.Colony(colony_params(capacity_hint=int(len(cells["x"]) * 1.5)))
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
+    col = device.Colony(colony_params(capacity_hint=int(len(cells["x"]) * 1.5), precision=prec))
     col.set_cells(cells)
     for _ in range(args.warmup):
         col.step()
@@ -352,9 +414,10 @@ def run_frozen(args):
     col.profiling(True)
     it, res, ms = col.bbpgd_frozen(3e-4, max(args.steps, 1))
     prof = col.profile()
-    m = int(round((prof["bbpgd_algo_bytes"] / max(prof["bbpgd_iterations"], 1) - 288.0 * n) / 312.0))
-    algo = it * (312.0 * m + 288.0 * n)
-    print(json.dumps({"frozen_bbpgd": True, "radius": args.radius, "cells": n, "constraints": m, "iterations": it,
+    bc, bn = ALGO_BYTES[args.precision]
+    m = int(round((prof["bbpgd_algo_bytes"] / max(prof["bbpgd_iterations"], 1) - bn * n) / bc))
+    algo = it * (bc * m + bn * n)
+    print(json.dumps({"frozen_bbpgd": True, "precision": args.precision, "radius": args.radius, "cells": n, "constraints": m, "iterations": it,
                       "residual": res, "ms_per_solve": ms, "algo_bytes_per_solve": algo,
                       "algo_gbs": algo / (ms / 1e3) / 1e9,
                       "frac_of_hbm": algo / (ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"]}), flush=True)
@@ -397,12 +460,19 @@ def run_jobs(args):
         jobs = colony_jobs(len(arr), rng, args.r_min, args.r_max, args.hard_frac, arr)
     else:
         jobs = colony_jobs(args.jobs, rng, args.r_min, args.r_max, args.hard_frac)
-    res, wall = device.serve(jobs, slots=args.slots, hbm_budget_bytes=args.hbm_budget)
+    for j in jobs:
+        j["params"].max_bbpgd_iterations = args.max_bbpgd
+    res, wall = device.serve(jobs, slots=args.slots, hbm_budget_bytes=args.hbm_budget, check=False)
+    failed = [dict(job=k, status=abi.STATUS_NAMES.get(r["status"], r["status"]), steps=r["steps"], cells=r["cells"],
+                   radius=r["radius"], dt=r["dt"], r_end=jobs[k]["end_radius"], hard=jobs[k]["hard"],
+                   tau=jobs[k]["params"].tau, max_step_bbpgd=r["max_step_bbpgd"])
+              for k, r in enumerate(res) if r["status"] != 0]
     lat = np.array([r["finish_s"] - r["arrival_s"] for r in res])
     cells = sum(r["cell_steps"] for r in res)
     sample = [dict(j, arrival_s=0.0) for j in jobs[: args.baseline_jobs]]
-    res1, wall1 = device.serve(sample, slots=1, hbm_budget_bytes=args.hbm_budget)
-    same = all(a["checksum"] == b["checksum"] and a["steps"] == b["steps"] for a, b in zip(res1, res))
+    res1, wall1 = device.serve(sample, slots=1, hbm_budget_bytes=args.hbm_budget, check=False)
+    same = all(a["checksum"] == b["checksum"] and a["steps"] == b["steps"] and a["status"] == b["status"]
+               for a, b in zip(res1, res))
     seq_rate = sum(r["cell_steps"] for r in res1) / wall1
     line = {
         "metric": METRIC, "mode": "serve" if args.rate > 0 else "batch",
@@ -414,6 +484,8 @@ def run_jobs(args):
         "one_at_a_time": {"jobs": len(sample), "cell_steps_per_s": seq_rate, "wall_s": wall1},
         "speedup_vs_one_at_a_time": (cells / wall) / seq_rate,
         "results_identical_alone_and_in_mix": same,
+        "max_step_bbpgd": int(max(r["max_step_bbpgd"] for r in res)),
+        "failed_jobs": failed,
         "config": {"r_end": [args.r_min, args.r_max], "growth_rate": [0.5, 1.5], "hard_fraction": args.hard_frac,
                    "hbm_budget_bytes": args.hbm_budget, "tolerance": 1e-3, "dtype": "f64"},
     }
@@ -428,6 +500,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--radius", type=float, default=RADIUS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
+                    help="BBPGD operand precision (mixed: FP32 D/L/M/U, FP64 gamma, dots, residual)")
     ap.add_argument("--verbose", action="store_true", help="per-step solver statistics on stderr")
     ap.add_argument("--frozen", action="store_true", help="BBPGD microbench on a frozen constraint set")
     ap.add_argument("--jobs", type=int, default=0, help="batch sweep of N colonies (continuous batching)")
@@ -440,6 +514,7 @@ def main():
     ap.add_argument("--hbm-budget", type=float, default=150e9)
     ap.add_argument("--baseline-jobs", type=int, default=8)
     ap.add_argument("--job-seed", type=int, default=0)
+    ap.add_argument("--max-bbpgd", type=int, default=500000, help="BBPGD iteration cap of each job")
     args = ap.parse_args()
     if args.jobs > 0 or args.rate > 0:
         run_jobs(args)

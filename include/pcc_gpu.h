@@ -63,6 +63,12 @@ typedef int pcc_status;
 #define PCC_GHOSTS_SINGLE_RANK 1
 
 #define PCC_PRECISION_FP64 0
+/* Mixed precision (planar colonies): the BBPGD operands D, L, M and U and the
+ * D / M products in FP32; gamma, the gradient, Phi, the stress sums, the BB dot
+ * products, the residual, positions and orientations in FP64.  Contact
+ * geometry stays FP64, so the contact set is the FP64 one.  Non-planar
+ * colonies run the FP64 solver. */
+#define PCC_PRECISION_MIXED 1
 
 /* Mirrors SimulationParameters (util/Config.h:27-56, defaults in
  * util/CLIParser.h:296-365) plus the run-time switches of this library. */
@@ -91,7 +97,7 @@ typedef struct pcc_params {
   double dt_cap;                       /* > 0: adapted dt never exceeds this */
   int ghost_mode;                      /* PCC_GHOSTS_* */
   unsigned long long seed;             /* seeds the division length draws */
-  int precision;                       /* PCC_PRECISION_FP64 */
+  int precision;                       /* PCC_PRECISION_FP64 or PCC_PRECISION_MIXED */
   long long capacity_hint;             /* expected peak cell count (0: grow on demand) */
   int solver_variant;                  /* PCC_SOLVER_AUTO or PCC_SOLVER_GENERAL */
 } pcc_params;
@@ -148,7 +154,7 @@ typedef struct pcc_profile {
   long long bbpgd_launches;     /* persistent BBPGD kernel launches */
   long long bbpgd_iterations;   /* iterations they ran */
   double bbpgd_ms;              /* device time of those launches */
-  double bbpgd_algo_bytes;      /* sum over launches of iterations * (312 C + 288 N) */
+  double bbpgd_algo_bytes;      /* sum over launches of iterations * (312 C + 288 N); (192 C + 144 N) mixed */
   double detect_ms;             /* contact detection + incidence lists */
   double solve_ms;              /* whole pcc_solve calls */
   long long solves;
@@ -243,6 +249,9 @@ typedef struct pcc_job_result {
   double arrival_s, start_s, finish_s;  /* seconds after the start of pcc_serve */
   double footprint_bytes;      /* projected device footprint used for admission */
   double checksum;             /* sum over final cells of x+y+z+q0+q1+q2+q3+length */
+  long long max_step_bbpgd;    /* most BBPGD iterations in one step */
+  double radius;               /* colony radius after the last step */
+  double dt;                   /* time step of the last step */
 } pcc_job_result;
 
 /* Continuous batching of independent colonies (no counterpart in the

@@ -30,6 +30,8 @@ MODE_HARD = 0
 MODE_SOFT = 1
 GHOSTS_NONE = 0
 GHOSTS_SINGLE_RANK = 1
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
 SOLVER_AUTO = 0
 SOLVER_GENERAL = 1
 
@@ -130,6 +132,9 @@ class JobResult(C.Structure):
         ("finish_s", C.c_double),
         ("footprint_bytes", C.c_double),
         ("checksum", C.c_double),
+        ("max_step_bbpgd", C.c_longlong),
+        ("radius", C.c_double),
+        ("dt", C.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -266,6 +266,7 @@ pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out) {
   *out = nullptr;
   if (params->temperature > 0) return PCC_ERR_INVALID;  // Brownian kicks are not on the device path
   if (params->mode != PCC_MODE_HARD && params->mode != PCC_MODE_SOFT) return PCC_ERR_INVALID;
+  if (params->precision != PCC_PRECISION_FP64 && params->precision != PCC_PRECISION_MIXED) return PCC_ERR_INVALID;
   if (!(params->linked_cell_size > 0) || !(params->xi > 0) || !(params->tau > 0)) return PCC_ERR_INVALID;
   pcc_ctx* ctx = new (std::nothrow) pcc_ctx();
   if (!ctx) return PCC_ERR_NOMEM;
@@ -274,7 +275,15 @@ pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out) {
   cudaError_t e = cudaSetDevice(device);
   if (!e) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (!e) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-  if (!e) e = cudaMalloc(&ctx->status, sizeof(DevStatus));
+  if (!e) {
+    // keep freed stream-ordered blocks cached in the process (no return to
+    // the driver at every synchronisation)
+    cudaMemPool_t pool;
+    unsigned long long keep_all = ~0ULL;
+    e = cudaDeviceGetDefaultMemPool(&pool, device);
+    if (!e) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+  }
+  if (!e) e = cudaMallocAsync(&ctx->status, sizeof(DevStatus), ctx->stream);
   if (!e) e = cudaMallocHost(&ctx->status_host, sizeof(DevStatus));
   if (!e) e = cudaMallocHost(&ctx->pinned_ll, 64 * sizeof(long long));
   if (!e) e = cudaMemsetAsync(ctx->status, 0, sizeof(DevStatus), ctx->stream);
@@ -295,12 +304,15 @@ pcc_status pcc_destroy(pcc_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
-  if (ctx->status) cudaFree(ctx->status);
+  if (ctx->status) cudaFreeAsync(ctx->status, ctx->stream);
   if (ctx->status_host) cudaFreeHost(ctx->status_host);
   if (ctx->pinned_ll) cudaFreeHost(ctx->pinned_ll);
   cudaStream_t s = ctx->stream;
-  delete ctx;
-  if (s) cudaStreamDestroy(s);
+  delete ctx;  // device buffers are freed on the context's stream
+  if (s) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
   return PCC_OK;
 }
 

@@ -14,33 +14,36 @@
 
 namespace pcc {
 
-// Growable device buffer.  grow() keeps the first `keep` elements.
+// Growable device buffer in stream-ordered memory: growth allocates, copies
+// the first `keep` elements and frees the old block on the owning stream, so
+// it never synchronises the device (colonies that grow side by side in one
+// process keep running while another reallocates).
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t cap = 0;
+  cudaStream_t owner = nullptr;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, owner);
   }
   cudaError_t reserve(size_t n, size_t keep, cudaStream_t s) {
     if (n <= cap) return cudaSuccess;
     size_t nc = cap ? cap : 64;
     while (nc < n) nc = nc + nc / 2 + 64;
     T* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, nc * sizeof(T));
+    cudaError_t e = cudaMallocAsync(&q, nc * sizeof(T), s);
     if (e != cudaSuccess) return e;
     if (p && keep) {
       e = cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s);
       if (e != cudaSuccess) return e;
-      e = cudaStreamSynchronize(s);
-      if (e != cudaSuccess) return e;
     }
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
     p = q;
     cap = nc;
+    owner = s;
     return cudaSuccess;
   }
 };
@@ -116,6 +119,9 @@ struct pcc_ctx {
   pcc::DevBuf<int2> p_ij;
   pcc::DevBuf<double2> p_n, p_t, p_s;
   pcc::DevBuf<double4> p_st0, p_st1, p_inc, p_cell, p_u;
+  // ... their FP32 forms (mixed precision)
+  pcc::DevBuf<float2> pf_n, pf_t, pf_s;
+  pcc::DevBuf<float4> pf_inc, pf_cell, pf_u;
   bool planar = false;  // set by the last binning pass
 
   // step scratch
@@ -136,6 +142,7 @@ struct pcc_ctx {
   long long launches = 0;
   int coop_blocks = 0;         // co-resident blocks of the general solver kernel
   int coop_blocks_planar = 0;  // ... of the planar one
+  int coop_blocks_mixed = 0;   // ... of its mixed-precision form
 
   bool profiling = false;
   pcc_profile prof{};

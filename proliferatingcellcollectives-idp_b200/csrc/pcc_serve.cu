@@ -76,15 +76,18 @@ void run_job(const pcc_job& job, int device, Clock::time_point t0, pcc_job_resul
     const long long cap = job.max_steps > 0 ? job.max_steps : (1LL << 62);
     long long bb = 0;
     while (st.colony_radius < job.end_radius && steps < cap) {
+      pcc_get_dt(ctx, &r->dt);
       rc = pcc_step(ctx, &st);
       if (rc != PCC_OK) break;
       cs += (double)st.n_cells;
       bb += st.bbpgd_iterations;
+      if (st.bbpgd_iterations > r->max_step_bbpgd) r->max_step_bbpgd = st.bbpgd_iterations;
+      r->radius = st.colony_radius;
       ++steps;
     }
     r->bbpgd_iterations = bb;
   }
-  if (rc == PCC_OK) {
+  if (ctx) {
     size_t n = 0;
     pcc_cell_count(ctx, &n);
     std::vector<double> buf(10 * (n + 1));
@@ -101,7 +104,7 @@ void run_job(const pcc_job& job, int device, Clock::time_point t0, pcc_job_resul
     o.length = p + 7 * (n + 1);
     o.l0 = p + 8 * (n + 1);
     o.diameter = p + 9 * (n + 1);
-    rc = pcc_download_cells(ctx, &o, n, &n);
+    if (pcc_download_cells(ctx, &o, n, &n) != PCC_OK) n = 0;
     double sum = 0;
     for (size_t i = 0; i < n; ++i)
       sum += o.x[i] + o.y[i] + o.z[i] + o.q0[i] + o.q1[i] + o.q2[i] + o.q3[i] + o.length[i];

@@ -381,21 +381,48 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
 // every other term of the general kernel is an exact zero, and a running sum
 // that starts at +0 is unchanged by adding a signed zero, so skipping them
 // gives bit-identical results.  Operands are packed so each gather is one
-// 32-byte sector:
+// sector:
 //   per incidence entry  inc  = (D_x, D_y, D_t, s) of that side,
 //   per constraint       st   = (gamma, g, gamma_old, 0), ping-pong per iteration,
 //                        ij, n = (n_x, n_y), t = (t_iz, t_jz), s = (s_i, s_j),
 //   per cell             cell = (M_lin, M_rot, len, ldot_prev), u = (u_x, u_y, w_z, dldot).
+// Real = double is the plain FP64 method.  Real = float is the mixed-precision
+// form: the D, L and M entries, U and the D / M products are FP32 (half the
+// operand bytes), while gamma, the gradient, Phi / phi_next, the stress sum
+// sigma = L^T gamma, the BB dot products and the residual stay FP64.
+template <class Real>
+struct PlanarTypes;
+template <>
+struct PlanarTypes<double> {
+  using V2 = double2;
+  using V4 = double4;
+};
+template <>
+struct PlanarTypes<float> {
+  using V2 = float2;
+  using V4 = float4;
+};
+
+__device__ __forceinline__ double4 mk4(double a, double b, double c, double d, double*) {
+  return make_double4(a, b, c, d);
+}
+__device__ __forceinline__ float4 mk4(double a, double b, double c, double d, float*) {
+  return make_float4((float)a, (float)b, (float)c, (float)d);
+}
+
+template <class Real>
 struct PlanarArgs {
+  using V2 = typename PlanarTypes<Real>::V2;
+  using V4 = typename PlanarTypes<Real>::V4;
   long long m, n;
   const int2* ij;
-  const double2 *nn, *tt, *ss;
+  const V2 *nn, *tt, *ss;
   double* phi;    // Phi on entry, phi_next on exit
   double* gamma;  // gamma_0 on entry, gamma_{k-1} on exit
   double4* st[2];
   const int *inc_off, *inc_ent;
-  const double4 *inc, *cell;
-  double4* u;
+  const V4 *inc, *cell;
+  V4* u;
   double *U, *F, *sig, *ldot, *imp;  // general-layout outputs on residual iterations
   double dt, lambda, tau, tol;
   long long max_it;
@@ -405,28 +432,47 @@ struct PlanarArgs {
   DevStatus* st_err;
 };
 
-__device__ __forceinline__ void planar_cell_pass(const PlanarArgs& a, long long p, int mode, const double4* stp,
-                                                 double alpha, bool final) {
-  double f0 = 0.0, f1 = 0.0, f5 = 0.0, sg = 0.0;
+template <class Real>
+__device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long long p, int mode,
+                                                 const double4* stp, double alpha, bool final) {
+  constexpr bool kF64 = sizeof(Real) == 8;
+  Real f0 = 0, f1 = 0, f5 = 0;
+  double sg = 0.0;
   const int b = a.inc_off[p], e = a.inc_off[p + 1];
   for (int k = b; k < e; ++k) {
     const long long c = a.inc_ent[k] >> 1;
-    const double4 d = a.inc[k];
+    const auto d = a.inc[k];
     const double4 s = ldcg(stp + c);
     const double gc = mode == 0 ? s.z : project(s.x, s.y, alpha);
     const double diff = sub(gc, s.z);
-    f0 = add(f0, mul(d.x, diff));
-    f1 = add(f1, mul(d.y, diff));
-    f5 = add(f5, mul(d.z, diff));
-    sg = add(sg, mul(d.w, gc));
+    if constexpr (kF64) {
+      f0 = add(f0, mul(d.x, diff));
+      f1 = add(f1, mul(d.y, diff));
+      f5 = add(f5, mul(d.z, diff));
+      sg = add(sg, mul(d.w, gc));
+    } else {
+      const float df = (float)diff;
+      f0 = fmaf(d.x, df, f0);
+      f1 = fmaf(d.y, df, f1);
+      f5 = fmaf(d.z, df, f5);
+      sg = fma((double)d.w, gc, sg);
+    }
   }
-  const double4 cl = a.cell[p];
-  const double ux = add(add(0.0, mul(cl.x, f0)), 0.0);
-  const double uy = add(add(0.0, mul(cl.x, f1)), 0.0);
-  const double wz = add(add(0.0, mul(cl.y, f5)), 0.0);
+  const auto cl = a.cell[p];
+  double ux, uy, wz;
+  const double ldp = cl.w;
+  if constexpr (kF64) {
+    ux = add(add(0.0, mul(cl.x, f0)), 0.0);
+    uy = add(add(0.0, mul(cl.x, f1)), 0.0);
+    wz = add(add(0.0, mul(cl.y, f5)), 0.0);
+  } else {
+    ux = cl.x * f0;
+    uy = cl.x * f1;
+    wz = cl.y * f5;
+  }
   const double im = exp(vscale(-a.lambda, sg));
-  const double ld = vscale(dvd(1.0, a.tau), mul(cl.z, im));
-  a.u[p] = make_double4(ux, uy, wz, sub(ld, cl.w));
+  const double ld = vscale(dvd(1.0, a.tau), mul((double)cl.z, im));
+  a.u[p] = mk4(ux, uy, wz, sub(ld, ldp), (Real*)nullptr);
   if (final) {
     double* U = a.U + 6 * p;
     double* F = a.F + 6 * p;
@@ -448,24 +494,40 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs& a, long long 
   }
 }
 
-__device__ __forceinline__ double planar_grad(const PlanarArgs& a, long long c) {
+template <class Real>
+__device__ __forceinline__ double planar_grad(const PlanarArgs<Real>& a, long long c) {
   const int2 ij = a.ij[c];
-  const double2 n = a.nn[c], t = a.tt[c], s = a.ss[c];
-  const double4 ui = ldcg(a.u + ij.x), uj = ldcg(a.u + ij.y);
-  double pd = 0.0;  // gi < gj: the i block comes first in column order
-  pd = add(pd, mul(n.x, ui.x));
-  pd = add(pd, mul(n.y, ui.y));
-  pd = add(pd, mul(t.x, ui.z));
-  pd = add(pd, mul(-n.x, uj.x));
-  pd = add(pd, mul(-n.y, uj.y));
-  pd = add(pd, mul(t.y, uj.z));
-  double gr = 0.0;
-  gr = add(gr, mul(s.x, ui.w));
-  gr = add(gr, mul(s.y, uj.w));
-  return add(a.phi[c], add(mul(a.dt, pd), mul(-a.dt, gr)));
+  const auto n = a.nn[c];
+  const auto t = a.tt[c];
+  const auto s = a.ss[c];
+  const auto ui = ldcg(a.u + ij.x);
+  const auto uj = ldcg(a.u + ij.y);
+  if constexpr (sizeof(Real) == 8) {
+    double pd = 0.0;  // gi < gj: the i block comes first in column order
+    pd = add(pd, mul(n.x, ui.x));
+    pd = add(pd, mul(n.y, ui.y));
+    pd = add(pd, mul(t.x, ui.z));
+    pd = add(pd, mul(-n.x, uj.x));
+    pd = add(pd, mul(-n.y, uj.y));
+    pd = add(pd, mul(t.y, uj.z));
+    double gr = 0.0;
+    gr = add(gr, mul(s.x, ui.w));
+    gr = add(gr, mul(s.y, uj.w));
+    return add(a.phi[c], add(mul(a.dt, pd), mul(-a.dt, gr)));
+  } else {
+    float pd = n.x * ui.x;
+    pd = fmaf(n.y, ui.y, pd);
+    pd = fmaf(t.x, ui.z, pd);
+    pd = fmaf(-n.x, uj.x, pd);
+    pd = fmaf(-n.y, uj.y, pd);
+    pd = fmaf(t.y, uj.z, pd);
+    const float gr = fmaf(s.y, uj.w, s.x * ui.w);
+    return a.phi[c] + a.dt * ((double)pd - (double)gr);
+  }
 }
 
-__global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs a) {
+template <class Real>
+__global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
   __shared__ double sm[4 * kBlock];
   const unsigned nb = gridDim.x;
   const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
@@ -585,36 +647,53 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs a) {
 }
 
 // Packs the planar operands of one ReLCP phase.
-__global__ void k_pack_planar_cons(ConsView cs, long long m, int2* __restrict__ ij, double2* __restrict__ nn,
-                                   double2* __restrict__ tt, double2* __restrict__ ss, double4* __restrict__ st) {
+template <class V2>
+__device__ __forceinline__ V2 mk2(double a, double b);
+template <>
+__device__ __forceinline__ double2 mk2<double2>(double a, double b) {
+  return make_double2(a, b);
+}
+template <>
+__device__ __forceinline__ float2 mk2<float2>(double a, double b) {
+  return make_float2((float)a, (float)b);
+}
+
+template <class Real>
+__global__ void k_pack_planar_cons(ConsView cs, long long m, int2* __restrict__ ij,
+                                   typename PlanarTypes<Real>::V2* __restrict__ nn,
+                                   typename PlanarTypes<Real>::V2* __restrict__ tt,
+                                   typename PlanarTypes<Real>::V2* __restrict__ ss, double4* __restrict__ st) {
+  using V2 = typename PlanarTypes<Real>::V2;
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m) return;
   ij[c] = make_int2(cs.gi[c], cs.gj[c]);
-  nn[c] = make_double2(cs.nx[c], cs.ny[c]);
-  tt[c] = make_double2(cs.tiz[c], cs.tjz[c]);
-  ss[c] = make_double2(cs.si[c], cs.sj[c]);
+  nn[c] = mk2<V2>(cs.nx[c], cs.ny[c]);
+  tt[c] = mk2<V2>(cs.tiz[c], cs.tjz[c]);
+  ss[c] = mk2<V2>(cs.si[c], cs.sj[c]);
   const double g = cs.gamma[c];
   st[c] = make_double4(g, 0.0, g, 0.0);
 }
 
+template <class Real>
 __global__ void k_pack_planar_inc(ConsView cs, const int* __restrict__ inc_ent, long long ne,
-                                  double4* __restrict__ inc) {
+                                  typename PlanarTypes<Real>::V4* __restrict__ inc) {
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ne) return;
   const int ent = inc_ent[k];
   const long long c = ent >> 1;
   if ((ent & 1) == 0)
-    inc[k] = make_double4(cs.nx[c], cs.ny[c], cs.tiz[c], cs.si[c]);
+    inc[k] = mk4(cs.nx[c], cs.ny[c], cs.tiz[c], cs.si[c], (Real*)nullptr);
   else
-    inc[k] = make_double4(-cs.nx[c], -cs.ny[c], cs.tjz[c], cs.sj[c]);
+    inc[k] = mk4(-cs.nx[c], -cs.ny[c], cs.tjz[c], cs.sj[c], (Real*)nullptr);
 }
 
+template <class Real>
 __global__ void k_pack_planar_cells(const double* __restrict__ Ml, const double* __restrict__ Mr,
                                     const double* __restrict__ len, const double* __restrict__ ldot_prev, long long n,
-                                    double4* __restrict__ cell) {
+                                    typename PlanarTypes<Real>::V4* __restrict__ cell) {
   long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  cell[p] = make_double4(Ml[p], Mr[p], len[p], ldot_prev[p]);
+  cell[p] = mk4(Ml[p], Mr[p], len[p], ldot_prev[p], (Real*)nullptr);
 }
 
 // Cell update after a solve: dC = G U (Physics.cpp:220-265), Euler step and
@@ -859,75 +938,102 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   a.st = ctx->status;
 
   const bool planar = ctx->planar && ctx->params.solver_variant != PCC_SOLVER_GENERAL;
-  PlanarArgs pa;
+  const bool mixed = planar && ctx->params.precision == PCC_PRECISION_MIXED;
+  PlanarArgs<double> pa;
+  PlanarArgs<float> pf;
   if (planar) {
     const size_t ne = 2 * m;
-    if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_n.reserve(mm, 0, s)) || (e = ctx->p_t.reserve(mm, 0, s)) ||
-        (e = ctx->p_s.reserve(mm, 0, s)) || (e = ctx->p_st0.reserve(mm, 0, s)) || (e = ctx->p_st1.reserve(mm, 0, s)) ||
-        (e = ctx->p_inc.reserve(ne + 1, 0, s)) || (e = ctx->p_cell.reserve(nn, 0, s)) ||
-        (e = ctx->p_u.reserve(nn, 0, s)))
+    if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_st0.reserve(mm, 0, s)) || (e = ctx->p_st1.reserve(mm, 0, s)))
       return e;
+    if (mixed) {
+      if ((e = ctx->pf_n.reserve(mm, 0, s)) || (e = ctx->pf_t.reserve(mm, 0, s)) || (e = ctx->pf_s.reserve(mm, 0, s)) ||
+          (e = ctx->pf_inc.reserve(ne + 1, 0, s)) || (e = ctx->pf_cell.reserve(nn, 0, s)) ||
+          (e = ctx->pf_u.reserve(nn, 0, s)))
+        return e;
+    } else {
+      if ((e = ctx->p_n.reserve(mm, 0, s)) || (e = ctx->p_t.reserve(mm, 0, s)) || (e = ctx->p_s.reserve(mm, 0, s)) ||
+          (e = ctx->p_inc.reserve(ne + 1, 0, s)) || (e = ctx->p_cell.reserve(nn, 0, s)) ||
+          (e = ctx->p_u.reserve(nn, 0, s)))
+        return e;
+    }
     if (m) {
-      k_pack_planar_cons<<<grid_for((long long)m), kBlock, 0, s>>>(cv, (long long)m, ctx->p_ij.p, ctx->p_n.p,
-                                                                   ctx->p_t.p, ctx->p_s.p, ctx->p_st0.p);
-      k_pack_planar_inc<<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne, ctx->p_inc.p);
+      if (mixed) {
+        k_pack_planar_cons<float><<<grid_for((long long)m), kBlock, 0, s>>>(
+            cv, (long long)m, ctx->p_ij.p, ctx->pf_n.p, ctx->pf_t.p, ctx->pf_s.p, ctx->p_st0.p);
+        k_pack_planar_inc<float><<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne,
+                                                                             ctx->pf_inc.p);
+      } else {
+        k_pack_planar_cons<double><<<grid_for((long long)m), kBlock, 0, s>>>(
+            cv, (long long)m, ctx->p_ij.p, ctx->p_n.p, ctx->p_t.p, ctx->p_s.p, ctx->p_st0.p);
+        k_pack_planar_inc<double><<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne,
+                                                                              ctx->p_inc.p);
+      }
       ctx->launches += 2;
     }
     if (n) {
-      k_pack_planar_cells<<<grid_for((long long)n), kBlock, 0, s>>>(ctx->Mlin.p, ctx->Mrot.p, ctx->cells.len.p,
-                                                                    ctx->cells.ldot.p, (long long)n, ctx->p_cell.p);
+      if (mixed)
+        k_pack_planar_cells<float><<<grid_for((long long)n), kBlock, 0, s>>>(
+            ctx->Mlin.p, ctx->Mrot.p, ctx->cells.len.p, ctx->cells.ldot.p, (long long)n, ctx->pf_cell.p);
+      else
+        k_pack_planar_cells<double><<<grid_for((long long)n), kBlock, 0, s>>>(
+            ctx->Mlin.p, ctx->Mrot.p, ctx->cells.len.p, ctx->cells.ldot.p, (long long)n, ctx->p_cell.p);
       ctx->launches++;
     }
-    pa.m = (long long)m;
-    pa.n = (long long)n;
-    pa.ij = ctx->p_ij.p;
+    auto fill = [&](auto& q) {
+      q.m = (long long)m;
+      q.n = (long long)n;
+      q.ij = ctx->p_ij.p;
+      q.phi = cv.sd;
+      q.gamma = cv.gamma;
+      q.st[0] = ctx->p_st0.p;
+      q.st[1] = ctx->p_st1.p;
+      q.inc_off = ctx->inc_off.p;
+      q.inc_ent = ctx->inc_ent.p;
+      q.U = ctx->U.p;
+      q.F = ctx->F.p;
+      q.sig = ctx->sig.p;
+      q.ldot = ctx->ldot_new.p;
+      q.imp = ctx->imp_new.p;
+      q.dt = dt;
+      q.lambda = ctx->params.lambda;
+      q.tau = ctx->params.tau;
+      q.tol = ctx->params.tolerance;
+      q.max_it = ctx->params.max_bbpgd_iterations;
+      q.partials = ctx->partials.p;
+      q.nchunks = nchunks;
+      q.sc = ctx->scal.p;
+      q.st_err = ctx->status;
+    };
+    fill(pa);
+    fill(pf);
     pa.nn = ctx->p_n.p;
     pa.tt = ctx->p_t.p;
     pa.ss = ctx->p_s.p;
-    pa.phi = cv.sd;
-    pa.gamma = cv.gamma;
-    pa.st[0] = ctx->p_st0.p;
-    pa.st[1] = ctx->p_st1.p;
-    pa.inc_off = ctx->inc_off.p;
-    pa.inc_ent = ctx->inc_ent.p;
     pa.inc = ctx->p_inc.p;
     pa.cell = ctx->p_cell.p;
     pa.u = ctx->p_u.p;
-    pa.U = ctx->U.p;
-    pa.F = ctx->F.p;
-    pa.sig = ctx->sig.p;
-    pa.ldot = ctx->ldot_new.p;
-    pa.imp = ctx->imp_new.p;
-    pa.dt = dt;
-    pa.lambda = ctx->params.lambda;
-    pa.tau = ctx->params.tau;
-    pa.tol = ctx->params.tolerance;
-    pa.max_it = ctx->params.max_bbpgd_iterations;
-    pa.partials = ctx->partials.p;
-    pa.nchunks = nchunks;
-    pa.sc = ctx->scal.p;
-    pa.st_err = ctx->status;
+    pf.nn = ctx->pf_n.p;
+    pf.tt = ctx->pf_t.p;
+    pf.ss = ctx->pf_s.p;
+    pf.inc = ctx->pf_inc.p;
+    pf.cell = ctx->pf_cell.p;
+    pf.u = ctx->pf_u.p;
   }
-  int& coop = planar ? ctx->coop_blocks_planar : ctx->coop_blocks;
+  const void* kern = mixed ? (const void*)k_bbpgd_planar<float>
+                           : planar ? (const void*)k_bbpgd_planar<double> : (const void*)k_bbpgd;
+  int& coop = mixed ? ctx->coop_blocks_mixed : planar ? ctx->coop_blocks_planar : ctx->coop_blocks;
   if (coop == 0) {
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, planar ? (const void*)k_bbpgd_planar
-                                                                           : (const void*)k_bbpgd,
-                                                           kBlock, 0)))
-      return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0))) return e;
     coop = per_sm * ctx->num_sms;
   }
   long long want = (long long)grid_for((long long)n);
   if (nchunks > want) want = nchunks;
   if (want > coop) want = coop;
   if (want < 1) want = 1;
-  void* args[] = {&a};
-  void* pargs[] = {&pa};
+  void* args[] = {mixed ? (void*)&pf : planar ? (void*)&pa : (void*)&a};
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], s);
-  if (planar)
-    e = cudaLaunchCooperativeKernel((void*)k_bbpgd_planar, dim3((unsigned)want), dim3(kBlock), pargs, 0, s);
-  else
-    e = cudaLaunchCooperativeKernel((void*)k_bbpgd, dim3((unsigned)want), dim3(kBlock), args, 0, s);
+  e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)want), dim3(kBlock), args, 0, s);
   ctx->launches++;
   if (e) return e;
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);
@@ -943,7 +1049,9 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     ctx->prof.bbpgd_launches++;
     ctx->prof.bbpgd_iterations += host.iterations;
     ctx->prof.bbpgd_ms += ms;
-    ctx->prof.bbpgd_algo_bytes += (double)host.iterations * (312.0 * (double)m + 288.0 * (double)n);
+    // 312 B per constraint and 288 B per cell in FP64; the FP32 operand terms halve
+    const double bc = mixed ? 192.0 : 312.0, bn = mixed ? 144.0 : 288.0;
+    ctx->prof.bbpgd_algo_bytes += (double)host.iterations * (bc * (double)m + bn * (double)n);
   }
   if (ctx->status_host->flags) {
     *status = (ctx->status_host->flags & kDevErrTimeout) ? PCC_ERR_TIMEOUT : PCC_ERR_BOUNDS;

@@ -201,11 +201,11 @@ class Colony:
         return int(self.lib.pcc_launch_count(self.h))
 
 
-def serve(jobs: list[dict], slots: int, hbm_budget_bytes: float = 150e9, device: int = 0):
+def serve(jobs: list[dict], slots: int, hbm_budget_bytes: float = 150e9, device: int = 0, check: bool = True):
     """Runs colony jobs with continuous batching (pcc_serve).  Each job is a
     dict with 'params' (abi.Params), 'end_radius' and optional 'arrival_s',
-    'max_steps'.  Returns (list of result dicts, wall seconds); raises
-    PccError if a job failed."""
+    'max_steps'.  Returns (list of result dicts, wall seconds); with check,
+    raises PccError if a job failed (else each result carries its status)."""
     lib = load_library()
     n = len(jobs)
     arr = (abi.Job * max(n, 1))()
@@ -218,7 +218,7 @@ def serve(jobs: list[dict], slots: int, hbm_budget_bytes: float = 150e9, device:
     wall = C.c_double(0)
     rc = lib.pcc_serve(arr, n, int(slots), float(hbm_budget_bytes), device, res, C.byref(wall))
     out = [res[i].as_dict() for i in range(n)]
-    if rc != 0:
+    if rc != 0 and (check or rc in (abi.PCC_ERR_INVALID, abi.PCC_ERR_CAPACITY)):
         raise PccError(rc, _REFERENCE_MESSAGES.get(rc, f"pcc_serve: {abi.STATUS_NAMES.get(rc, rc)}"))
     return out, wall.value
 

@@ -58,6 +58,8 @@ def test_create_rejects_bad_parameters():
     assert lib.pcc_create(C.byref(p), 0, C.byref(h)) == abi.PCC_ERR_INVALID
     p = abi.default_params(linked_cell_size=0.0)
     assert lib.pcc_create(C.byref(p), 0, C.byref(h)) == abi.PCC_ERR_INVALID
+    p = abi.default_params(precision=7)
+    assert lib.pcc_create(C.byref(p), 0, C.byref(h)) == abi.PCC_ERR_INVALID
 
 
 def test_null_context_is_rejected():

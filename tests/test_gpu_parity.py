@@ -278,3 +278,36 @@ def test_num_constraints_match_reference(name):
     g.set_cells(sub(fx, "cells_"))
     g.solve(p.dt, 0)
     np.testing.assert_array_equal(g.get_cells()["num_constraints"], fx["solve_cells_num_constraints"])
+
+
+@pytest.mark.parametrize("name", ["hard_r10_seed3", "hard_tight_r10_seed3"])
+def test_mixed_precision_solve_close_to_fp64(name):
+    """Mixed precision (FP32 D, L, M, U; FP64 gamma, BB dots, residual) meets
+    the same LCP tolerance, and moves cells within 1e-5 of the FP64 path."""
+    fx = load_fixture(name)
+    out = []
+    for prec in (abi.PRECISION_FP64, abi.PRECISION_MIXED):
+        p = params_of(fx, precision=prec)
+        g = Colony(p)
+        g.set_cells(sub(fx, "cells_"))
+        st = g.solve(p.dt, 0)
+        out.append((st, g.get_cells(), g.constraints()))
+    (s64, c64, k64), (s32, c32, k32) = out
+    tol = params_of(fx).tolerance
+    assert s32["residual"] <= tol and s32["max_overlap"] <= tol
+    assert np.all(k32["gamma"] >= 0.0)
+    d = cells_max_diff(c64, c32)
+    assert max(d.values()) < 1e-5, d
+    assert s32["bbpgd_iterations"] > 0
+
+
+def test_mixed_precision_trajectory_matches_reference():
+    fx = load_fixture("traj_hard_seed3_3000")
+    p = params_of(fx, precision=abi.PRECISION_MIXED)
+    g = Colony(p)
+    g.set_cells(sub(fx, "start_"))
+    hist = [g.step() for _ in range(len(fx["hist_n_cells"]))]
+    np.testing.assert_array_equal([h["n_cells"] for h in hist], fx["hist_n_cells"])
+    assert all(h["max_overlap"] <= p.tolerance for h in hist)
+    d = cells_max_diff(g.get_cells(), sub(fx, "final_"))
+    assert max(d.values()) < 5e-3, d
