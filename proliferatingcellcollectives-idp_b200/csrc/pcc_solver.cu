@@ -439,6 +439,7 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long
   Real f0 = 0, f1 = 0, f5 = 0;
   double sg = 0.0;
   const int b = a.inc_off[p], e = a.inc_off[p + 1];
+#pragma unroll 4
   for (int k = b; k < e; ++k) {
     const long long c = a.inc_ent[k] >> 1;
     const auto d = a.inc[k];
@@ -538,14 +539,16 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
   if (!barrier(sc, nb, a.st_err)) return;
   for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
     double v[4] = {0, 0, 0, 0};
+#pragma unroll
     for (int k = 0; k < kPerThread; ++k) {
-      long long c = ch * kChunk + k * kBlock + threadIdx.x;
-      if (c >= a.m) break;
-      const double g = planar_grad(a, c);
-      const double gm = a.st[0][c].x;
-      a.st[0][c].y = g;
-      double r = proj_grad_abs(g, gm);
-      v[3] = v[3] < r ? r : v[3];
+      const long long c = ch * kChunk + k * kBlock + threadIdx.x;
+      if (c < a.m) {
+        const double g = planar_grad(a, c);
+        const double gm = a.st[0][c].x;
+        a.st[0][c].y = g;
+        double r = proj_grad_abs(g, gm);
+        v[3] = v[3] < r ? r : v[3];
+      }
     }
     block_reduce4(v, sm);
     if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
@@ -577,20 +580,22 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
     if (!barrier(sc, nb, a.st_err)) return;
     for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
       double v[4] = {0, 0, 0, 0};
+#pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
-        long long c = ch * kChunk + k * kBlock + threadIdx.x;
-        if (c >= a.m) break;
-        const double4 s = ldcg(sp + c);
-        const double gam = project(s.x, s.y, alpha);
-        const double g = planar_grad(a, c);
-        so[c] = make_double4(gam, g, s.z, 0.0);
-        const double dgm = sub(gam, s.x), dg = sub(g, s.y);
-        v[0] = add(v[0], mul(dgm, dgm));
-        v[1] = add(v[1], mul(dgm, dg));
-        v[2] = add(v[2], mul(dg, dg));
-        if (check) {
-          double r = proj_grad_abs(g, gam);
-          v[3] = v[3] < r ? r : v[3];
+        const long long c = ch * kChunk + k * kBlock + threadIdx.x;
+        if (c < a.m) {
+          const double4 s = ldcg(sp + c);
+          const double gam = project(s.x, s.y, alpha);
+          const double g = planar_grad(a, c);
+          so[c] = make_double4(gam, g, s.z, 0.0);
+          const double dgm = sub(gam, s.x), dg = sub(g, s.y);
+          v[0] = add(v[0], mul(dgm, dgm));
+          v[1] = add(v[1], mul(dgm, dg));
+          v[2] = add(v[2], mul(dg, dg));
+          if (check) {
+            double r = proj_grad_abs(g, gam);
+            v[3] = v[3] < r ? r : v[3];
+          }
         }
       }
       block_reduce4(v, sm);
