@@ -100,6 +100,8 @@ typedef struct pcc_params {
   int precision;                       /* PCC_PRECISION_FP64 or PCC_PRECISION_MIXED */
   long long capacity_hint;             /* expected peak cell count (0: grow on demand) */
   int solver_variant;                  /* PCC_SOLVER_AUTO or PCC_SOLVER_GENERAL */
+  double log_every_colony_radius_delta;  /* VTK output cadence of the driver (CLI default 0.5) */
+  double log_every_sim_time_delta;       /* ... and by simulated time (CLI default 100000) */
 } pcc_params;
 
 /* BBPGD kernel choice.  A planar colony (every z = 0, rotation about z only)
@@ -264,6 +266,64 @@ typedef struct pcc_job_result {
  * mix.  Returns the first failing job's status (all results are filled). */
 pcc_status pcc_serve(const pcc_job* jobs, size_t n_jobs, int slots, double hbm_budget_bytes, int device,
                      pcc_job_result* results, double* wall_s);
+
+/* ---- VTK output and restart (the reference's file formats, one rank) ---- */
+
+/* The per-log record of vtk::SimulationStep (logger/SimulationLogger.h:7-30);
+ * field names and order as the reference writes them. */
+typedef struct pcc_sim_record {
+  double simulation_time_s;
+  double time_since_last_log_s;
+  unsigned long long step;
+  int num_particles;
+  unsigned long long num_constraints;
+  double colony_radius;
+  int recursive_iterations;
+  unsigned long long bbpgd_iterations;
+  double max_overlap;
+  double residual;
+  double dt_s;
+  double memory_usage_mb;
+  double peak_memory_mb;
+  double cpu_time_s;
+  double mpi_comm_time_s;
+  double load_imbalance;
+} pcc_sim_record;
+
+/* Writes one particle file pair, <outdir>/data/<prefix>_<index, 7 digits>_rank_0000.vtu
+ * and <outdir>/<prefix>_<index>.pvtu, byte-identical to vtk::ParticleLogger::log
+ * (logger/ParticleLogger.cpp:13-76, logger/VTK.h) at one rank for the same
+ * cells.  With ghost_copies, writes the self-ghost copies of the single-rank
+ * decomposition instead (Domain::exchangeGhostParticles, spatial/Domain.cpp:339-403),
+ * as copies carry them: no force, velocity, impedance, stress or contact count. */
+pcc_status pcc_vtk_write_particles(const char* outdir, const char* prefix, unsigned long long index,
+                                   const pcc_cells* cells, size_t n, int ghost_copies);
+/* simulation_<index> files of vtk::SimulationLogger::log (logger/SimulationLogger.cpp:9-36). */
+pcc_status pcc_vtk_write_simulation(const char* outdir, unsigned long long index, const pcc_sim_record* rec);
+/* parameters_<index> files of vtk::ParameterLogger::log (logger/ParameterLogger.cpp:11-40). */
+pcc_status pcc_vtk_write_parameters(const char* outdir, unsigned long long index, const pcc_params* params);
+
+/* Asynchronous log point of Domain::run (spatial/Domain.cpp:188-200): snapshots
+ * the resident cells on the device, in stream order after the last step, and
+ * returns; a background thread copies the snapshot to the host and writes the
+ * particles_, ghost_particles_ and (rec != NULL) simulation_ files of `index`
+ * while the colony keeps stepping.  pcc_log_vtk_wait blocks until every
+ * pending write is on disk and reports a failed write. */
+pcc_status pcc_log_vtk(pcc_ctx* ctx, const char* outdir, unsigned long long index, const pcc_sim_record* rec);
+pcc_status pcc_log_vtk_wait(pcc_ctx* ctx);
+
+/* Restart (-starter_vtk): vtk::VTKStateLoader::loadLatestState
+ * (loader/VTKStateLoader.cpp:24-162) on a VTK output directory (or a file in
+ * it): the latest simulation_ record and the particles of the same index.
+ * Cells come back as the loader builds them (l0 = 1, diameter 0.5, age 1,
+ * no torque; force and velocities from the file, positions at the file's
+ * float precision).  With out = NULL only *n (and the clock) are returned;
+ * PCC_ERR_CAPACITY if cap < *n.  dt is the file's dt_s field, which the
+ * reference reads but does not use. */
+pcc_status pcc_vtk_load(const char* vtk_path, pcc_cells* out, size_t cap, size_t* n, double* sim_time,
+                        long long* step, double* dt);
+/* Sets the simulated time and the step counter of a context (after a restart). */
+pcc_status pcc_set_clock(pcc_ctx* ctx, double sim_time, long long iteration);
 
 /* The CUDA stream all work of the context is queued on (a cudaStream_t). */
 void* pcc_get_stream(const pcc_ctx* ctx);

@@ -46,6 +46,8 @@
 #undef private
 #undef protected
 #include "dynamics/Constraint.h"
+#include "loader/VTKStateLoader.h"
+#include "logger/SimulationLogger.h"
 #include "pcc_gpu.h"
 #include "simulation/Particle.h"
 #include "simulation/ParticleManager.h"
@@ -340,6 +342,82 @@ int pcc_ref_get_constraints(void* h, pcc_contacts* out, size_t cap, size_t* n) {
   if (cap < *n) return PCC_ERR_CAPACITY;
   export_constraints(c->last_constraints, out);
   return 0;
+}
+
+// The log point of Domain::run (spatial/Domain.cpp:192-196) on the current
+// state: particles, ghost particles and the simulation record, written by the
+// reference's loggers under <outdir>/vtk_output_<mode>.
+int pcc_ref_log_vtk(void* h, const pcc_sim_record* r) {
+  auto* c = static_cast<RefColony*>(h);
+  std::error_code ec;
+  auto cwd = std::filesystem::current_path();
+  std::filesystem::current_path(c->outdir, ec);
+  if (ec) return PCC_ERR_INVALID;
+  Domain& d = *c->domain;
+  d.particle_logger_->log(d.particle_manager_->local_particles);
+  d.ghost_particle_logger_->log(d.particle_manager_->ghost_particles);
+  vtk::SimulationStep st{};
+  st.simulation_time_s = r->simulation_time_s;
+  st.time_since_last_log_s = r->time_since_last_log_s;
+  st.step = (size_t)r->step;
+  st.num_particles = r->num_particles;
+  st.num_constraints = (size_t)r->num_constraints;
+  st.colony_radius = r->colony_radius;
+  st.recursive_iterations = r->recursive_iterations;
+  st.bbpgd_iterations = (size_t)r->bbpgd_iterations;
+  st.max_overlap = r->max_overlap;
+  st.residual = r->residual;
+  st.dt_s = r->dt_s;
+  st.memory_usage_mb = r->memory_usage_mb;
+  st.peak_memory_mb = r->peak_memory_mb;
+  st.cpu_time_s = r->cpu_time_s;
+  st.mpi_comm_time_s = r->mpi_comm_time_s;
+  st.load_imbalance = r->load_imbalance;
+  d.simulation_logger_->log(st);
+  std::filesystem::current_path(cwd, ec);
+  return 0;
+}
+
+// vtk::VTKStateLoader::loadLatestState on a VTK output directory: the cells
+// as the loader builds them (global ids in file order).
+int pcc_ref_load_vtk(const char* dir, pcc_cells* out, size_t cap, size_t* n, double* sim_time, long long* step,
+                     double* dt) {
+  try {
+    vtk::VTKStateLoader loader(dir);
+    auto state = loader.loadLatestState();
+    *n = state.particles.size();
+    if (sim_time) *sim_time = state.simulation_time_s;
+    if (step) *step = state.step;
+    if (dt) *dt = state.dt_s;
+    if (!out) return 0;
+    if (cap < *n) return PCC_ERR_CAPACITY;
+    for (size_t i = 0; i < *n; ++i) {
+      const Particle& p = state.particles[i];
+      const auto& d = p.getData();
+      out->x[i] = d.position[0];
+      out->y[i] = d.position[1];
+      out->z[i] = d.position[2];
+      out->q0[i] = d.quaternion[0];
+      out->q1[i] = d.quaternion[1];
+      out->q2[i] = d.quaternion[2];
+      out->q3[i] = d.quaternion[3];
+      out->length[i] = d.length;
+      out->l0[i] = d.l0;
+      out->diameter[i] = d.diameter;
+      if (out->age) out->age[i] = d.age;
+      if (out->force) {
+        for (int k = 0; k < 3; ++k) out->force[6 * i + k] = p.getForce()[k];
+        for (int k = 0; k < 3; ++k) out->force[6 * i + 3 + k] = p.getTorque()[k];
+      }
+      if (out->velocity) {
+        for (int k = 0; k < 3; ++k) out->velocity[6 * i + k] = p.getVelocityLinear()[k];
+        for (int k = 0; k < 3; ++k) out->velocity[6 * i + 3 + k] = p.getVelocityAngular()[k];
+      }
+    }
+    return 0;
+  } catch (const std::exception&) {
+    return PCC_ERR_INVALID;
+  }
 }
 
 double pcc_ref_get_dt(void* h) { return static_cast<RefColony*>(h)->params.sim_config.dt_s; }

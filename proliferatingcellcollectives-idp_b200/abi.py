@@ -63,6 +63,8 @@ class Params(C.Structure):
         ("precision", C.c_int),
         ("capacity_hint", C.c_longlong),
         ("solver_variant", C.c_int),
+        ("log_every_colony_radius_delta", C.c_double),
+        ("log_every_sim_time_delta", C.c_double),
     ]
 
 
@@ -141,6 +143,27 @@ class JobResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SimRecord(C.Structure):
+    _fields_ = [
+        ("simulation_time_s", C.c_double),
+        ("time_since_last_log_s", C.c_double),
+        ("step", C.c_ulonglong),
+        ("num_particles", C.c_int),
+        ("num_constraints", C.c_ulonglong),
+        ("colony_radius", C.c_double),
+        ("recursive_iterations", C.c_int),
+        ("bbpgd_iterations", C.c_ulonglong),
+        ("max_overlap", C.c_double),
+        ("residual", C.c_double),
+        ("dt_s", C.c_double),
+        ("memory_usage_mb", C.c_double),
+        ("peak_memory_mb", C.c_double),
+        ("cpu_time_s", C.c_double),
+        ("mpi_comm_time_s", C.c_double),
+        ("load_imbalance", C.c_double),
+    ]
+
+
 def default_params(**over) -> Params:
     """Reference defaults (code/cpp/src/util/CLIParser.h:296-365), hard mode."""
     p = Params()
@@ -166,6 +189,8 @@ def default_params(**over) -> Params:
     p.precision = 0
     p.capacity_hint = 0
     p.solver_variant = 0
+    p.log_every_colony_radius_delta = 0.5
+    p.log_every_sim_time_delta = 100000.0
     for k, v in over.items():
         if k == "lambda":
             k = "lambda_"

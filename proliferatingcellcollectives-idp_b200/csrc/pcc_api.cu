@@ -259,6 +259,8 @@ void pcc_default_params(pcc_params* p) {
   p->cfl_factor = 0.5;
   p->mode = PCC_MODE_HARD;
   p->ghost_mode = PCC_GHOSTS_SINGLE_RANK;
+  p->log_every_colony_radius_delta = 0.5;
+  p->log_every_sim_time_delta = 100000;
 }
 
 pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out) {
@@ -301,6 +303,12 @@ pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out) {
 pcc_status pcc_destroy(pcc_ctx* ctx) {
   if (!ctx) return PCC_OK;
   cudaSetDevice(ctx->device);
+  vtk_writer_shutdown(ctx);
+  if (ctx->vtk_stream) {
+    cudaStreamSynchronize(ctx->vtk_stream);
+    cudaStreamDestroy(ctx->vtk_stream);
+  }
+  if (ctx->vtk_ev) cudaEventDestroy(ctx->vtk_ev);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);

@@ -79,6 +79,8 @@ struct SolverScalars {
 
 }  // namespace pcc
 
+struct pcc_vtk_writer_state;
+
 struct pcc_ctx {
   pcc_params params{};
   int device = 0;
@@ -143,6 +145,13 @@ struct pcc_ctx {
   int coop_blocks = 0;         // co-resident blocks of the general solver kernel
   int coop_blocks_planar = 0;  // ... of the planar one
   int coop_blocks_mixed = 0;   // ... of its mixed-precision form
+
+  // VTK output: device snapshot, side stream and background writer
+  pcc::DevBuf<double> vtk_dev;
+  pcc::DevBuf<int> vtk_idev;
+  cudaStream_t vtk_stream = nullptr;
+  cudaEvent_t vtk_ev = nullptr;
+  pcc_vtk_writer_state* vtk_writer = nullptr;
 
   bool profiling = false;
   pcc_profile prof{};

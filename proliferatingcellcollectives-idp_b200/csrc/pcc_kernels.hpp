@@ -48,4 +48,8 @@ cudaError_t colony_radius(pcc_ctx* ctx, double* out);
 cudaError_t adapt_dt(pcc_ctx* ctx);  // updates ctx->params.dt
 cudaError_t mobility(pcc_ctx* ctx);
 
+// ---- pcc_vtk.cu
+// Waits for and stops the context's VTK writer thread.
+void vtk_writer_shutdown(pcc_ctx* ctx);
+
 }  // namespace pcc

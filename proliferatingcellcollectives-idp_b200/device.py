@@ -58,6 +58,14 @@ def load_library(path: str | os.PathLike | None = None):
     lib.pcc_launch_count.argtypes = [VP]
     lib.pcc_division_seed.restype = C.c_uint
     lib.pcc_division_seed.argtypes = [C.c_ulonglong, C.c_ulonglong]
+    lib.pcc_vtk_write_particles.argtypes = [C.c_char_p, C.c_char_p, C.c_ulonglong, P(abi.Cells), C.c_size_t, C.c_int]
+    lib.pcc_vtk_write_simulation.argtypes = [C.c_char_p, C.c_ulonglong, P(abi.SimRecord)]
+    lib.pcc_vtk_write_parameters.argtypes = [C.c_char_p, C.c_ulonglong, P(abi.Params)]
+    lib.pcc_log_vtk.argtypes = [VP, C.c_char_p, C.c_ulonglong, P(abi.SimRecord)]
+    lib.pcc_log_vtk_wait.argtypes = [VP]
+    lib.pcc_vtk_load.argtypes = [C.c_char_p, P(abi.Cells), C.c_size_t, P(C.c_size_t), P(C.c_double),
+                                 P(C.c_longlong), P(C.c_double)]
+    lib.pcc_set_clock.argtypes = [VP, C.c_double, C.c_longlong]
     lib.pcc_division_length_host.restype = C.c_double
     lib.pcc_division_length_host.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_double]
     _LIB = lib
@@ -192,6 +200,20 @@ class Colony:
         self._check(self.lib.pcc_get_profile(self.h, C.byref(pr)), "profile")
         return pr.as_dict()
 
+    # VTK output / restart
+    def log_vtk(self, outdir: str, index: int, record: dict | None = None):
+        """Queue a log point (particles_, ghost_particles_ and, with a record,
+        simulation_ files of `index`); returns before the files are written."""
+        rec = sim_record(record) if record is not None else None
+        self._check(self.lib.pcc_log_vtk(self.h, str(outdir).encode(), int(index),
+                                         C.byref(rec) if rec is not None else None), "log_vtk")
+
+    def log_vtk_wait(self):
+        self._check(self.lib.pcc_log_vtk_wait(self.h), "log_vtk_wait")
+
+    def set_clock(self, sim_time: float, iteration: int):
+        self._check(self.lib.pcc_set_clock(self.h, float(sim_time), int(iteration)), "set_clock")
+
     @property
     def stream(self) -> int:
         return int(self.lib.pcc_get_stream(self.h) or 0)
@@ -225,3 +247,50 @@ def serve(jobs: list[dict], slots: int, hbm_budget_bytes: float = 150e9, device:
 
 def division_length(seed: int, k: int, length: float) -> float:
     return load_library().pcc_division_length_host(seed, k, length)
+
+
+def sim_record(d: dict) -> abi.SimRecord:
+    r = abi.SimRecord()
+    for k, v in d.items():
+        setattr(r, k, v)
+    return r
+
+
+def write_particles(outdir: str, prefix: str, index: int, cells: dict, ghost_copies: bool = False):
+    """Host-only writer of a particle file pair in the reference's format."""
+    n = len(cells["x"])
+    ca = abi.CellArrays.from_dict(cells)
+    rc = load_library().pcc_vtk_write_particles(str(outdir).encode(), prefix.encode(), int(index),
+                                                C.byref(ca.struct), n, 1 if ghost_copies else 0)
+    if rc != 0:
+        raise PccError(rc, "pcc_vtk_write_particles failed")
+
+
+def write_simulation(outdir: str, index: int, record: dict):
+    rc = load_library().pcc_vtk_write_simulation(str(outdir).encode(), int(index), C.byref(sim_record(record)))
+    if rc != 0:
+        raise PccError(rc, "pcc_vtk_write_simulation failed")
+
+
+def write_parameters(outdir: str, index: int, params: abi.Params):
+    rc = load_library().pcc_vtk_write_parameters(str(outdir).encode(), int(index), C.byref(params))
+    if rc != 0:
+        raise PccError(rc, "pcc_vtk_write_parameters failed")
+
+
+def load_vtk(path: str):
+    """Restart state from a VTK output directory (or a file in it):
+    (cells dict, simulation time, step, dt) as pcc_vtk_load returns them."""
+    lib = load_library()
+    n = C.c_size_t(0)
+    t, dt = C.c_double(0), C.c_double(0)
+    step = C.c_longlong(0)
+    rc = lib.pcc_vtk_load(str(path).encode(), None, 0, C.byref(n), C.byref(t), C.byref(step), C.byref(dt))
+    if rc != 0:
+        raise PccError(rc, f"pcc_vtk_load: cannot read a VTK state from {path}")
+    ca = abi.CellArrays(int(n.value))
+    rc = lib.pcc_vtk_load(str(path).encode(), C.byref(ca.struct), ca.cap, C.byref(n), C.byref(t), C.byref(step),
+                          C.byref(dt))
+    if rc != 0:
+        raise PccError(rc, f"pcc_vtk_load: cannot read a VTK state from {path}")
+    return ca.to_dict(int(n.value)), t.value, int(step.value), dt.value

@@ -161,11 +161,43 @@ class RefColony(_CpuColony):
             _bind_common(lib, self.prefix)
             lib.pcc_ref_division_length.restype = C.c_double
             lib.pcc_ref_division_length.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_double]
+            lib.pcc_ref_log_vtk.argtypes = [_VP, _P(abi.SimRecord)]
+            lib.pcc_ref_load_vtk.argtypes = [C.c_char_p, _P(abi.Cells), C.c_size_t, _P(C.c_size_t),
+                                             _P(C.c_double), _P(C.c_longlong), _P(C.c_double)]
             _REF_LIBS[name] = lib
         self.lib = _REF_LIBS[name]
         self.n_cells_hint = 1024
         self._tmp = tempfile.mkdtemp(prefix="pccref_") if outdir is None else outdir
+        self._mode = params.mode
         self.h = self.lib.pcc_ref_create(C.byref(params), self._tmp.encode())
+
+
+    @property
+    def vtk_dir(self) -> Path:
+        """Where the reference's loggers write (Domain's ./vtk_output_<mode>)."""
+        return Path(self._tmp) / "vtk_output_hard" if self._mode == 0 else Path(self._tmp) / "vtk_output_soft"
+
+    def log_vtk(self, record: abi.SimRecord):
+        rc = self.lib.pcc_ref_log_vtk(self.h, C.byref(record))
+        if rc != 0:
+            raise RuntimeError("pcc_ref_log_vtk failed")
+
+
+def ref_load_vtk(path: str):
+    """The reference's VTKStateLoader on a directory: (cells, time, step, dt)."""
+    if "libpccref_strict.so" not in _REF_LIBS:
+        RefColony(abi.default_params())
+    lib = _REF_LIBS["libpccref_strict.so"]
+    n = C.c_size_t(0)
+    t, dt = C.c_double(0), C.c_double(0)
+    step = C.c_longlong(0)
+    if lib.pcc_ref_load_vtk(str(path).encode(), None, 0, C.byref(n), C.byref(t), C.byref(step), C.byref(dt)):
+        raise RuntimeError("reference loader failed")
+    ca = abi.CellArrays(int(n.value))
+    if lib.pcc_ref_load_vtk(str(path).encode(), C.byref(ca.struct), ca.cap, C.byref(n), C.byref(t), C.byref(step),
+                            C.byref(dt)):
+        raise RuntimeError("reference loader failed")
+    return ca.to_dict(int(n.value)), t.value, int(step.value), dt.value
 
 
 def ref_division_length(seed: int, k: int, length: float) -> float:

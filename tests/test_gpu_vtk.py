@@ -1,0 +1,62 @@
+"""VTK log points of a device colony: the asynchronous snapshot writer
+(pcc_log_vtk) against the host writer on the same state, and a restart from
+the written files."""
+from __future__ import annotations
+
+import filecmp
+
+import numpy as np
+import pytest
+
+from helpers import load_fixture, params_of, sub
+from pcc_b200 import device
+from pcc_b200.device import Colony
+
+pytestmark = pytest.mark.gpu
+
+RECORD = dict(simulation_time_s=0.5, time_since_last_log_s=0.25, step=7, num_particles=256, num_constraints=2654,
+              colony_radius=10.5, recursive_iterations=4, bbpgd_iterations=130, max_overlap=3.5e-4,
+              residual=1e-4, dt_s=0.001, memory_usage_mb=1.0, peak_memory_mb=2.0, cpu_time_s=3.0,
+              mpi_comm_time_s=4.0, load_imbalance=1.0)
+
+
+def test_async_log_matches_host_writer(tmp_path):
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx)
+    g = Colony(p)
+    g.set_cells(sub(fx, "cells_"))
+    g.solve(p.dt, 0)
+    states = []
+    for k in range(2):
+        states.append(g.get_cells())
+        g.log_vtk(str(tmp_path / "dev"), k, RECORD)
+        g.step()  # the colony steps on while the snapshot is written
+    g.log_vtk_wait()
+    for k, cells in enumerate(states):
+        device.write_particles(str(tmp_path / "host"), "particles", k, cells)
+        device.write_particles(str(tmp_path / "host"), "ghost_particles", k, cells, ghost_copies=True)
+        device.write_simulation(str(tmp_path / "host"), k, RECORD)
+        for pre in ("particles", "ghost_particles", "simulation"):
+            base = f"{pre}_{k:07d}"
+            assert filecmp.cmp(tmp_path / "dev" / f"{base}.pvtu", tmp_path / "host" / f"{base}.pvtu", shallow=False)
+            assert filecmp.cmp(tmp_path / "dev" / "data" / f"{base}_rank_0000.vtu",
+                               tmp_path / "host" / "data" / f"{base}_rank_0000.vtu", shallow=False), base
+
+
+def test_restart_from_logged_state(tmp_path):
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx)
+    g = Colony(p)
+    g.set_cells(sub(fx, "cells_"))
+    g.step()
+    before = g.get_cells()
+    g.log_vtk(str(tmp_path), 0, RECORD)
+    g.log_vtk_wait()
+    cells, t, step, dt = device.load_vtk(str(tmp_path))
+    assert (t, step) == (0.5, 7)
+    assert np.max(np.abs(cells["x"] - before["x"])) < 1e-4
+    h = Colony(p)
+    h.set_cells(cells)
+    h.set_clock(t, step)
+    st = h.step()
+    assert st["n_cells"] >= len(cells["x"]) and st["max_overlap"] <= p.tolerance
