@@ -102,6 +102,7 @@ typedef struct pcc_params {
   int solver_variant;                  /* PCC_SOLVER_AUTO or PCC_SOLVER_GENERAL */
   double log_every_colony_radius_delta;  /* VTK output cadence of the driver (CLI default 0.5) */
   double log_every_sim_time_delta;       /* ... and by simulated time (CLI default 100000) */
+  int log_bbpgd_trace;                   /* -log_bbgd_trace: trace BBPGD on every 10th step */
 } pcc_params;
 
 /* BBPGD kernel choice.  A planar colony (every z = 0, rotation about z only)
@@ -322,6 +323,33 @@ pcc_status pcc_log_vtk_wait(pcc_ctx* ctx);
  * reference reads but does not use. */
 pcc_status pcc_vtk_load(const char* vtk_path, pcc_cells* out, size_t cap, size_t* n, double* sim_time,
                         long long* step, double* dt);
+/* BBPGD trace (-log_bbgd_trace; solver/BBPGD.cpp:55-81, logger/BBPGDLogger.cpp,
+ * HardModelGradient::energy, HardModelGradient.cpp:160-203).  On a hard-model
+ * solve whose step counter is a multiple of 10, with params.log_bbpgd_trace
+ * set, the solver evaluates and tests the residual at every iteration (as the
+ * reference does while tracing) and records, per iteration, the residual, the
+ * step size and the energy terms; after the ReLCP loop the records are written
+ * as bbpgdtrace_<index> files (index from 1; earlier bbpgdtrace files in the
+ * directory are removed first, as the reference's logger does) into the
+ * trace directory, "logs" by default. */
+typedef struct pcc_bbpgd_trace_step {
+  unsigned long long step;                /* BBPGD iteration */
+  unsigned long long recursive_iteration; /* ReLCP phase */
+  unsigned long long total_constraints;
+  double residual;
+  double step_size;
+  double linear;     /* gamma . Phi */
+  double quadratic;  /* dt/2 gamma^T D^T M D gamma */
+  double growth;     /* dt/(lambda tau) sum l exp(-lambda L^T gamma) */
+  double total;
+} pcc_bbpgd_trace_step;
+pcc_status pcc_set_trace_dir(pcc_ctx* ctx, const char* dir);
+/* Writes trace records as bbpgdtrace_<first_index + k> files (host only). */
+pcc_status pcc_vtk_write_trace(const char* outdir, unsigned long long first_index, const pcc_bbpgd_trace_step* steps,
+                               size_t n);
+/* Records of the last traced solve (n = 0 if none); out = NULL returns n. */
+pcc_status pcc_get_bbpgd_trace(const pcc_ctx* ctx, pcc_bbpgd_trace_step* out, size_t cap, size_t* n);
+
 /* Sets the simulated time and the step counter of a context (after a restart). */
 pcc_status pcc_set_clock(pcc_ctx* ctx, double sim_time, long long iteration);
 

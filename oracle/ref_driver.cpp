@@ -104,7 +104,7 @@ void fill_params(SimulationParameters& sp, const pcc_params* p) {
   sp.sim_config.end_radius = p->end_radius;
   sp.sim_config.log_every_sim_time_delta = 0;
   sp.sim_config.log_every_colony_radius_delta = 0;
-  sp.sim_config.log_bbgd_trace = false;
+  sp.sim_config.log_bbgd_trace = p->log_bbpgd_trace != 0;
   sp.sim_config.min_box_size = {p->l0 + 1, p->l0 + 1, 0};
   sp.physics_config.xi = p->xi;
   sp.physics_config.TAU = p->tau;
@@ -231,6 +231,17 @@ int pcc_ref_solve(void* h, double dt, int iter, pcc_step_stats* st) {
     d.rebalance();
     exchange_ghosts(c);
   };
+  // a BBPGD trace is written to ./logs: run inside the scratch folder
+  std::error_code ec;
+  auto cwd = std::filesystem::current_path();
+  std::filesystem::current_path(c->outdir, ec);
+  struct Back {
+    std::filesystem::path p;
+    ~Back() {
+      std::error_code e2;
+      std::filesystem::current_path(p, e2);
+    }
+  } back{cwd};
   try {
     auto sol = d.particle_manager_->step(iter, fn);
     c->last_constraints = std::move(sol.constraints);

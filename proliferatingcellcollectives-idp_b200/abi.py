@@ -65,6 +65,7 @@ class Params(C.Structure):
         ("solver_variant", C.c_int),
         ("log_every_colony_radius_delta", C.c_double),
         ("log_every_sim_time_delta", C.c_double),
+        ("log_bbpgd_trace", C.c_int),
     ]
 
 
@@ -138,6 +139,15 @@ class JobResult(C.Structure):
         ("radius", C.c_double),
         ("dt", C.c_double),
     ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TraceStep(C.Structure):
+    _fields_ = [("step", C.c_ulonglong), ("recursive_iteration", C.c_ulonglong), ("total_constraints", C.c_ulonglong),
+                ("residual", C.c_double), ("step_size", C.c_double), ("linear", C.c_double),
+                ("quadratic", C.c_double), ("growth", C.c_double), ("total", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

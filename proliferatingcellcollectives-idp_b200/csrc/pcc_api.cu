@@ -131,9 +131,16 @@ void profile_detect(pcc_ctx* ctx) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
   } while (0)
 
-pcc_status solve_hard(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
+pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
   const double tol = ctx->params.tolerance;
   int phase = 0;
+  // BBPGD trace on every 10th step (dynamics/models/Hard.cpp:107-111); a new
+  // logger clears the earlier trace files
+  ctx->trace_active = ctx->params.log_bbpgd_trace && iter % 10 == 0;
+  if (ctx->trace_active) {
+    ctx->trace_host.clear();
+    vtk_clear_prefix(ctx->trace_dir, "bbpgdtrace");
+  }
   long long total_it = 0;
   double res = 0.0, max_ov = 0.0;
   ctx->ncons = 0;
@@ -155,6 +162,7 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
     profile_detect(ctx);
     long long it = 0;
     int status = 0;
+    ctx->trace_phase = phase;
     CU(bbpgd_solve(ctx, dt, &it, &res, &status), "bbpgd");
     total_it += it;
     if (status == PCC_ERR_NOCONV_BBPGD) return fail(ctx, status, "BBPGD did not converge");
@@ -164,6 +172,13 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
     }
     CU(apply_hard_solution(ctx, dt), "move");
     ++phase;
+  }
+  if (ctx->trace_active) {
+    ctx->trace_active = false;
+    // BBPGDLogger("logs", "bbpgdtrace", true): the third argument lands on the
+    // logger's starting index, so files count from 1 (logger/BBPGDLogger.h:23-27)
+    if (!vtk_write_trace(ctx->trace_dir, 1, ctx->trace_host))
+      return fail(ctx, PCC_ERR_INVALID, "cannot write the BBPGD trace files");
   }
   CU(grow_cells(ctx, dt), "grow");
   pcc_status rc = check_device(ctx, "hard step");
@@ -422,14 +437,13 @@ pcc_status pcc_download_cells(pcc_ctx* ctx, pcc_cells* c, size_t cap, size_t* n)
 }
 
 pcc_status pcc_solve(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* out) {
-  (void)iter;
   if (!ctx || !(dt > 0)) return PCC_ERR_INVALID;
   cudaSetDevice(ctx->device);
   pcc_step_stats st;
   std::memset(&st, 0, sizeof st);
   if (ctx->profiling) cudaEventRecord(ctx->ev[4], ctx->stream);
   if (ctx->n) CU(cudaMemsetAsync(ctx->cells.ncons.p, 0, ctx->n * sizeof(int), ctx->stream), "reset");  // Particle::reset
-  pcc_status rc = ctx->params.mode == PCC_MODE_SOFT ? solve_soft(ctx, dt, &st) : solve_hard(ctx, dt, &st);
+  pcc_status rc = ctx->params.mode == PCC_MODE_SOFT ? solve_soft(ctx, dt, &st) : solve_hard(ctx, dt, iter, &st);
   st.dt_used = dt;
   if (ctx->profiling) {
     cudaEventRecord(ctx->ev[5], ctx->stream);
@@ -622,6 +636,21 @@ pcc_status pcc_reset_profile(pcc_ctx* ctx) {
 pcc_status pcc_get_profile(const pcc_ctx* ctx, pcc_profile* out) {
   if (!ctx || !out) return PCC_ERR_INVALID;
   *out = ctx->prof;
+  return PCC_OK;
+}
+
+pcc_status pcc_set_trace_dir(pcc_ctx* ctx, const char* dir) {
+  if (!ctx || !dir || !*dir) return PCC_ERR_INVALID;
+  ctx->trace_dir = dir;
+  return PCC_OK;
+}
+
+pcc_status pcc_get_bbpgd_trace(const pcc_ctx* ctx, pcc_bbpgd_trace_step* out, size_t cap, size_t* n) {
+  if (!ctx || !n) return PCC_ERR_INVALID;
+  *n = ctx->trace_host.size();
+  if (!out) return PCC_OK;
+  if (cap < *n) return PCC_ERR_CAPACITY;
+  std::memcpy(out, ctx->trace_host.data(), *n * sizeof(pcc_bbpgd_trace_step));
   return PCC_OK;
 }
 

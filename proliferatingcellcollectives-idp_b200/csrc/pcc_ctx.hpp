@@ -153,6 +153,13 @@ struct pcc_ctx {
   cudaEvent_t vtk_ev = nullptr;
   pcc_vtk_writer_state* vtk_writer = nullptr;
 
+  // BBPGD trace of the current / last traced solve
+  bool trace_active = false;
+  int trace_phase = 0;
+  std::string trace_dir = "logs";
+  pcc::DevBuf<double> tr_part, trace_dev;
+  std::vector<pcc_bbpgd_trace_step> trace_host;
+
   bool profiling = false;
   pcc_profile prof{};
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

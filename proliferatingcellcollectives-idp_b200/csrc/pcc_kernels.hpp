@@ -51,5 +51,10 @@ cudaError_t mobility(pcc_ctx* ctx);
 // ---- pcc_vtk.cu
 // Waits for and stops the context's VTK writer thread.
 void vtk_writer_shutdown(pcc_ctx* ctx);
+// Removes <dir>/<prefix>*.pvtu and <dir>/data/<prefix>*.vtu (a new logger's reset).
+void vtk_clear_prefix(const std::string& dir, const std::string& prefix);
+// bbpgdtrace_<index> files of BBPGDLogger::log, indices first_index, first_index + 1, ...
+bool vtk_write_trace(const std::string& dir, unsigned long long first_index,
+                     const std::vector<pcc_bbpgd_trace_step>& steps);
 
 }  // namespace pcc

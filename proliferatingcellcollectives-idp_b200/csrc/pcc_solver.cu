@@ -47,7 +47,15 @@ struct SolverArgs {
   long long nchunks;
   SolverScalars* sc;
   DevStatus* st;
+  // BBPGD trace (-log_bbgd_trace): residual every iteration and the energy terms
+  int trace;
+  double* tr_part;     // 2 per block (cell terms), then 1 per chunk (linear term)
+  double* trace_out;   // kTraceWidth per iteration
+  long long trace_cap; // iterations that fit
 };
+
+constexpr int kTraceWidth = 8;  // it, residual, step size, linear, quadratic, growth, total, -
+
 
 // gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0): VecWAXPY with PETSc's special
 // cases for the coefficient, then VecPointwiseMax against 0.
@@ -141,8 +149,10 @@ __device__ __forceinline__ bool barrier_reduce(SolverScalars* sc, unsigned nbloc
 // (gam_prev, g_prev, alpha).  Writes U and dldot; with `final` also F, sigma,
 // ldot and impedance.
 __device__ __forceinline__ void cell_pass(const SolverArgs& a, long long p, int mode, const double* gprev_gam,
-                                          const double* gprev_g, double alpha, bool final) {
+                                          const double* gprev_g, double alpha, bool final, double* eq = nullptr,
+                                          double* eg = nullptr) {
   double F[6] = {0, 0, 0, 0, 0, 0};
+  double Fg[6] = {0, 0, 0, 0, 0, 0};  // D^T gamma (trace only)
   double sg = 0.0;
   const int b = a.inc_off[p], e = a.inc_off[p + 1];
   for (int k = b; k < e; ++k) {
@@ -171,6 +181,10 @@ __device__ __forceinline__ void cell_pass(const SolverArgs& a, long long p, int 
 #pragma unroll
     for (int q = 0; q < 6; ++q) F[q] = add(F[q], mul(D[q], diff));
     sg = add(sg, mul(side == 0 ? a.si[c] : a.sj[c], gc));
+    if (eq) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) Fg[q] = add(Fg[q], mul(D[q], gc));
+    }
   }
   const double ml = a.Mlin[p], mr = a.Mrot[p];
   double* U = a.U + 6 * p;
@@ -182,6 +196,11 @@ __device__ __forceinline__ void cell_pass(const SolverArgs& a, long long p, int 
   double im = exp(vscale(-a.lambda, sg));
   double ld = vscale(dvd(1.0, a.tau), mul(a.len[p], im));
   a.dl[p] = sub(ld, a.ldot_prev[p]);
+  if (eq) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) *eq = add(*eq, mul(Fg[q], mul(q < 3 ? ml : mr, Fg[q])));
+    *eg = add(*eg, mul(a.len[p], im));
+  }
   if (final) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) a.F[6 * p + q] = F[q];
@@ -249,6 +268,51 @@ __device__ __forceinline__ void block_reduce4(double v[4], double* sm) {
   __syncthreads();
 }
 
+// Energy of the BBPGD trace (HardModelGradient::energy, HardModelGradient.cpp:160-203)
+// from the block partials of the cell terms and the chunk partials of the
+// linear term; written by the last block of a barrier.
+__device__ __forceinline__ void trace_record(double* sm, const double* tr_part, unsigned nb, long long nchunks,
+                                             double dt, double lambda, double tau, long long it, double res,
+                                             double alpha, double* out, long long cap) {
+  double v[4] = {0, 0, 0, 0};
+  for (long long b = threadIdx.x; b < (long long)nb; b += kBlock) {
+    v[0] = add(v[0], ldcg(tr_part + 2 * b));
+    v[1] = add(v[1], ldcg(tr_part + 2 * b + 1));
+  }
+  for (long long ch = threadIdx.x; ch < nchunks; ch += kBlock) v[2] = add(v[2], ldcg(tr_part + 2 * nb + ch));
+  block_reduce4(v, sm);
+  if (threadIdx.x == 0 && it < cap) {
+    const double lin = v[2];
+    const double quad = mul(v[0], dvd(dt, 2.0));
+    const double growth = mul(v[1], dvd(dt, mul(lambda, tau)));
+    double* r = out + (long long)kTraceWidth * it;
+    r[0] = (double)it;
+    r[1] = res;
+    r[2] = alpha;
+    r[3] = lin;
+    r[4] = quad;
+    r[5] = growth;
+    r[6] = add(add(lin, quad), growth);
+    r[7] = 0.0;
+  }
+}
+
+// Block partials of the cell energy terms (all threads of the block call).
+__device__ __forceinline__ void trace_cells(double* sm, double eq, double eg, double* tr_part) {
+  double v[4] = {eq, eg, 0, 0};
+  block_reduce4(v, sm);
+  if (threadIdx.x == 0) {
+    tr_part[2 * blockIdx.x] = v[0];
+    tr_part[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
+__device__ __forceinline__ void trace_chunk(double* sm, double lin, double* tr_part, unsigned nb, long long ch) {
+  double v[4] = {lin, 0, 0, 0};
+  block_reduce4(v, sm);
+  if (threadIdx.x == 0) tr_part[2 * nb + ch] = v[0];
+}
+
 __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   __shared__ double sm[4 * kBlock];
   const unsigned nb = gridDim.x;
@@ -257,10 +321,16 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   SolverScalars* sc = a.sc;
 
   // ---- gradient at gamma_0 and the initial residual (BBPGD.cpp:40-44)
-  for (long long p = tid; p < a.n; p += stride) cell_pass(a, p, 0, nullptr, nullptr, 0.0, false);
+  {
+    double eq = 0.0, eg = 0.0;
+    for (long long p = tid; p < a.n; p += stride)
+      cell_pass(a, p, 0, nullptr, nullptr, 0.0, false, a.trace ? &eq : nullptr, &eg);
+    if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+  }
   if (!barrier(sc, nb, a.st)) return;
   for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
     double v[4] = {0, 0, 0, 0};
+    double lin = 0.0;
     for (int k = 0; k < kPerThread; ++k) {
       long long c = ch * kChunk + k * kBlock + threadIdx.x;
       if (c >= a.m) break;
@@ -270,9 +340,11 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
       a.gam[0][c] = gm;
       double r = proj_grad_abs(g, gm);
       v[3] = v[3] < r ? r : v[3];
+      if (a.trace) lin = add(lin, mul(gm, a.phi[c]));
     }
     block_reduce4(v, sm);
     if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
+    if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
   }
   auto reduce_init = [&]() {
     double v[4] = {0, 0, 0, 0};
@@ -287,6 +359,9 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
       sc->alpha = 1.0 / v[3];
       sc->converged = 0;
     }
+    if (a.trace)
+      trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
+                   a.trace_cap);
   };
   if (!barrier_reduce(sc, nb, a.st, reduce_init)) return;
 
@@ -294,15 +369,22 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   long long it = 1;
   while (it < a.max_it) {
     const double alpha = *(volatile double*)&sc->alpha;
-    const bool check = (it % 10) == 0;
+    // with the trace on the residual is evaluated (and tested) every iteration (BBPGD.cpp:73)
+    const bool check = (it % 10) == 0 || a.trace;
     const double* gp = a.gam[p];
     const double* gg = a.g[p];
     double* gc_out = a.gam[1 - p];
     double* g_out = a.g[1 - p];
-    for (long long q = tid; q < a.n; q += stride) cell_pass(a, q, 1, gp, gg, alpha, check);
+    {
+      double eq = 0.0, eg = 0.0;
+      for (long long q = tid; q < a.n; q += stride)
+        cell_pass(a, q, 1, gp, gg, alpha, check, a.trace ? &eq : nullptr, &eg);
+      if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+    }
     if (!barrier(sc, nb, a.st)) return;
     for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
       double v[4] = {0, 0, 0, 0};  // sum dgam^2, sum dgam*dg, sum dg^2, max residual
+      double lin = 0.0;
       for (int k = 0; k < kPerThread; ++k) {
         long long c = ch * kChunk + k * kBlock + threadIdx.x;
         if (c >= a.m) break;
@@ -319,6 +401,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
           double r = proj_grad_abs(g, gam);
           v[3] = v[3] < r ? r : v[3];
         }
+        if (a.trace) lin = add(lin, mul(gam, a.phi[c]));
       }
       block_reduce4(v, sm);
       if (threadIdx.x == 0) {
@@ -327,6 +410,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
         a.partials[4 * ch + 2] = v[2];
         a.partials[4 * ch + 3] = v[3];
       }
+      if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
     }
     auto reduce_iter = [&]() {
       double v[4] = {0, 0, 0, 0};
@@ -338,6 +422,9 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
         v[3] = v[3] < r ? r : v[3];
       }
       block_reduce4(v, sm);
+      if (a.trace)
+        trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, it, v[3], alpha, a.trace_out,
+                     a.trace_cap);
       if (threadIdx.x == 0) {
         int conv = 0;
         if (check) {
@@ -430,13 +517,19 @@ struct PlanarArgs {
   long long nchunks;
   SolverScalars* sc;
   DevStatus* st_err;
+  int trace;  // BBPGD trace, as in SolverArgs
+  double* tr_part;
+  double* trace_out;
+  long long trace_cap;
 };
 
 template <class Real>
 __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long long p, int mode,
-                                                 const double4* stp, double alpha, bool final) {
+                                                 const double4* stp, double alpha, bool final, double* eq = nullptr,
+                                                 double* eg = nullptr) {
   constexpr bool kF64 = sizeof(Real) == 8;
   Real f0 = 0, f1 = 0, f5 = 0;
+  double g0 = 0, g1 = 0, g5 = 0;  // D^T gamma (trace only)
   double sg = 0.0;
   const int b = a.inc_off[p], e = a.inc_off[p + 1];
 #pragma unroll 4
@@ -458,6 +551,11 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long
       f5 = fmaf(d.z, df, f5);
       sg = fma((double)d.w, gc, sg);
     }
+    if (eq) {
+      g0 = add(g0, mul((double)d.x, gc));
+      g1 = add(g1, mul((double)d.y, gc));
+      g5 = add(g5, mul((double)d.z, gc));
+    }
   }
   const auto cl = a.cell[p];
   double ux, uy, wz;
@@ -474,6 +572,11 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long
   const double im = exp(vscale(-a.lambda, sg));
   const double ld = vscale(dvd(1.0, a.tau), mul((double)cl.z, im));
   a.u[p] = mk4(ux, uy, wz, sub(ld, ldp), (Real*)nullptr);
+  if (eq) {
+    const double ml = cl.x, mr = cl.y;
+    *eq = add(*eq, add(add(mul(g0, mul(ml, g0)), mul(g1, mul(ml, g1))), mul(g5, mul(mr, g5))));
+    *eg = add(*eg, mul((double)cl.z, im));
+  }
   if (final) {
     double* U = a.U + 6 * p;
     double* F = a.F + 6 * p;
@@ -535,10 +638,16 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
   const long long stride = (long long)nb * kBlock;
   SolverScalars* sc = a.sc;
 
-  for (long long p = tid; p < a.n; p += stride) planar_cell_pass(a, p, 0, a.st[0], 0.0, false);
+  {
+    double eq = 0.0, eg = 0.0;
+    for (long long p = tid; p < a.n; p += stride)
+      planar_cell_pass(a, p, 0, a.st[0], 0.0, false, a.trace ? &eq : nullptr, &eg);
+    if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+  }
   if (!barrier(sc, nb, a.st_err)) return;
   for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
     double v[4] = {0, 0, 0, 0};
+    double lin = 0.0;
 #pragma unroll
     for (int k = 0; k < kPerThread; ++k) {
       const long long c = ch * kChunk + k * kBlock + threadIdx.x;
@@ -548,10 +657,12 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         a.st[0][c].y = g;
         double r = proj_grad_abs(g, gm);
         v[3] = v[3] < r ? r : v[3];
+        if (a.trace) lin = add(lin, mul(gm, a.phi[c]));
       }
     }
     block_reduce4(v, sm);
     if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
+    if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
   }
   auto reduce_init = [&]() {
     double v[4] = {0, 0, 0, 0};
@@ -566,6 +677,9 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
       sc->alpha = 1.0 / v[3];
       sc->converged = 0;
     }
+    if (a.trace)
+      trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
+                   a.trace_cap);
   };
   if (!barrier_reduce(sc, nb, a.st_err, reduce_init)) return;
 
@@ -573,13 +687,19 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
   long long it = 1;
   while (it < a.max_it) {
     const double alpha = *(volatile double*)&sc->alpha;
-    const bool check = (it % 10) == 0;
+    const bool check = (it % 10) == 0 || a.trace;
     const double4* sp = a.st[p];
     double4* so = a.st[1 - p];
-    for (long long q = tid; q < a.n; q += stride) planar_cell_pass(a, q, 1, sp, alpha, check);
+    {
+      double eq = 0.0, eg = 0.0;
+      for (long long q = tid; q < a.n; q += stride)
+        planar_cell_pass(a, q, 1, sp, alpha, check, a.trace ? &eq : nullptr, &eg);
+      if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+    }
     if (!barrier(sc, nb, a.st_err)) return;
     for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
       double v[4] = {0, 0, 0, 0};
+      double lin = 0.0;
 #pragma unroll
       for (int k = 0; k < kPerThread; ++k) {
         const long long c = ch * kChunk + k * kBlock + threadIdx.x;
@@ -596,6 +716,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
             double r = proj_grad_abs(g, gam);
             v[3] = v[3] < r ? r : v[3];
           }
+          if (a.trace) lin = add(lin, mul(gam, a.phi[c]));
         }
       }
       block_reduce4(v, sm);
@@ -605,6 +726,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         a.partials[4 * ch + 2] = v[2];
         a.partials[4 * ch + 3] = v[3];
       }
+      if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
     }
     auto reduce_iter = [&]() {
       double v[4] = {0, 0, 0, 0};
@@ -616,6 +738,9 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         v[3] = v[3] < r ? r : v[3];
       }
       block_reduce4(v, sm);
+      if (a.trace)
+        trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, it, v[3], alpha, a.trace_out,
+                     a.trace_cap);
       if (threadIdx.x == 0) {
         int conv = 0;
         if (check) {
@@ -941,6 +1066,19 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   a.nchunks = nchunks;
   a.sc = ctx->scal.p;
   a.st = ctx->status;
+  const bool tracing = ctx->trace_active;
+  long long trace_cap = 0;
+  if (tracing) {
+    trace_cap = ctx->params.max_bbpgd_iterations + 1;
+    if (trace_cap > (1LL << 22)) trace_cap = 1LL << 22;
+    if ((e = ctx->trace_dev.reserve((size_t)(kTraceWidth * trace_cap), 0, s))) return e;
+    // 2 per block of the largest grid, 1 per chunk
+    if ((e = ctx->tr_part.reserve((size_t)(2 * 8 * ctx->num_sms * 8 + nchunks + 1), 0, s))) return e;
+  }
+  a.trace = tracing ? 1 : 0;
+  a.tr_part = ctx->tr_part.p;
+  a.trace_out = ctx->trace_dev.p;
+  a.trace_cap = trace_cap;
 
   const bool planar = ctx->planar && ctx->params.solver_variant != PCC_SOLVER_GENERAL;
   const bool mixed = planar && ctx->params.precision == PCC_PRECISION_MIXED;
@@ -1008,6 +1146,10 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
       q.nchunks = nchunks;
       q.sc = ctx->scal.p;
       q.st_err = ctx->status;
+      q.trace = a.trace;
+      q.tr_part = a.tr_part;
+      q.trace_out = a.trace_out;
+      q.trace_cap = a.trace_cap;
     };
     fill(pa);
     fill(pf);
@@ -1048,6 +1190,28 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   if ((e = cudaStreamSynchronize(s))) return e;
   *iterations = host.iterations;
   *residual = host.residual;
+  if (tracing) {
+    // records 0 .. the last iteration run (BBPGD.cpp:55-81)
+    long long nrec = host.iterations + 1;
+    if (nrec > trace_cap) nrec = trace_cap;
+    std::vector<double> rec((size_t)(kTraceWidth * nrec));
+    if ((e = cudaMemcpy(rec.data(), ctx->trace_dev.p, rec.size() * sizeof(double), cudaMemcpyDeviceToHost)))
+      return e;
+    for (long long k = 0; k < nrec; ++k) {
+      const double* r = rec.data() + kTraceWidth * k;
+      pcc_bbpgd_trace_step t;
+      t.step = (unsigned long long)k;
+      t.recursive_iteration = (unsigned long long)ctx->trace_phase;
+      t.total_constraints = (unsigned long long)m;
+      t.residual = r[1];
+      t.step_size = r[2];
+      t.linear = r[3];
+      t.quadratic = r[4];
+      t.growth = r[5];
+      t.total = r[6];
+      ctx->trace_host.push_back(t);
+    }
+  }
   if (ctx->profiling) {
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);

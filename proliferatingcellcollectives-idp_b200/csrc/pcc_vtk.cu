@@ -546,6 +546,44 @@ bool read_vtu(const std::string& path, std::map<std::string, ArrayData>* out, st
 }
 
 }  // namespace vtkio
+
+void vtk_clear_prefix(const std::string& dir, const std::string& prefix) {
+  for (const std::string sub : {std::string(""), std::string("/data")}) {
+    const std::string d = dir + sub;
+    const char* ext = sub.empty() ? ".pvtu" : ".vtu";
+    const size_t el = std::strlen(ext);
+    if (DIR* dp = opendir(d.c_str())) {
+      std::vector<std::string> gone;
+      while (dirent* de = readdir(dp)) {
+        const std::string f = de->d_name;
+        if (f.size() > el && f.compare(f.size() - el, el, ext) == 0 && f.rfind(prefix, 0) == 0) gone.push_back(f);
+      }
+      closedir(dp);
+      for (const auto& f : gone) std::remove((d + "/" + f).c_str());
+    }
+  }
+}
+
+bool vtk_write_trace(const std::string& dir, unsigned long long first_index,
+                     const std::vector<pcc_bbpgd_trace_step>& steps) {
+  using namespace vtkio;
+  unsigned long long index = first_index;
+  for (const auto& t : steps) {
+    // BBPGDLogger::log (logger/BBPGDLogger.cpp:12-27): one file pair per record
+    const std::vector<Field> f = {fu("step", t.step),
+                                  fu("recursive_iteration", t.recursive_iteration),
+                                  fu("total_constraints", t.total_constraints),
+                                  fd("residual", t.residual),
+                                  fd("step_size", t.step_size),
+                                  fd("linear", t.linear),
+                                  fd("quadratic", t.quadratic),
+                                  fd("growth", t.growth),
+                                  fd("total", t.total)};
+    if (!write_files(dir, "bbpgdtrace", index++, f, "", 0, {})) return false;
+  }
+  return true;
+}
+
 }  // namespace pcc
 
 using namespace pcc;
@@ -618,6 +656,13 @@ pcc_status pcc_vtk_write_particles(const char* outdir, const char* prefix, unsig
 pcc_status pcc_vtk_write_simulation(const char* outdir, unsigned long long index, const pcc_sim_record* rec) {
   if (!outdir || !rec) return PCC_ERR_INVALID;
   return write_files(outdir, "simulation", index, simulation_fields(*rec), "", 0, {}) ? PCC_OK : PCC_ERR_INVALID;
+}
+
+pcc_status pcc_vtk_write_trace(const char* outdir, unsigned long long first_index, const pcc_bbpgd_trace_step* steps,
+                               size_t n) {
+  if (!outdir || (n && !steps)) return PCC_ERR_INVALID;
+  return vtk_write_trace(outdir, first_index, std::vector<pcc_bbpgd_trace_step>(steps, steps + n)) ? PCC_OK
+                                                                                                  : PCC_ERR_INVALID;
 }
 
 pcc_status pcc_vtk_write_parameters(const char* outdir, unsigned long long index, const pcc_params* p) {

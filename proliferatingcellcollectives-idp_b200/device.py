@@ -66,6 +66,9 @@ def load_library(path: str | os.PathLike | None = None):
     lib.pcc_vtk_load.argtypes = [C.c_char_p, P(abi.Cells), C.c_size_t, P(C.c_size_t), P(C.c_double),
                                  P(C.c_longlong), P(C.c_double)]
     lib.pcc_set_clock.argtypes = [VP, C.c_double, C.c_longlong]
+    lib.pcc_set_trace_dir.argtypes = [VP, C.c_char_p]
+    lib.pcc_get_bbpgd_trace.argtypes = [VP, P(abi.TraceStep), C.c_size_t, P(C.c_size_t)]
+    lib.pcc_vtk_write_trace.argtypes = [C.c_char_p, C.c_ulonglong, P(abi.TraceStep), C.c_size_t]
     lib.pcc_division_length_host.restype = C.c_double
     lib.pcc_division_length_host.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_double]
     _LIB = lib
@@ -211,6 +214,17 @@ class Colony:
     def log_vtk_wait(self):
         self._check(self.lib.pcc_log_vtk_wait(self.h), "log_vtk_wait")
 
+    def set_trace_dir(self, path: str):
+        self._check(self.lib.pcc_set_trace_dir(self.h, str(path).encode()), "set_trace_dir")
+
+    def bbpgd_trace(self) -> list[dict]:
+        """Records of the last traced hard-model solve (params.log_bbpgd_trace)."""
+        n = C.c_size_t(0)
+        self._check(self.lib.pcc_get_bbpgd_trace(self.h, None, 0, C.byref(n)), "trace")
+        arr = (abi.TraceStep * max(int(n.value), 1))()
+        self._check(self.lib.pcc_get_bbpgd_trace(self.h, arr, int(n.value), C.byref(n)), "trace")
+        return [arr[i].as_dict() for i in range(int(n.value))]
+
     def set_clock(self, sim_time: float, iteration: int):
         self._check(self.lib.pcc_set_clock(self.h, float(sim_time), int(iteration)), "set_clock")
 
@@ -294,3 +308,14 @@ def load_vtk(path: str):
     if rc != 0:
         raise PccError(rc, f"pcc_vtk_load: cannot read a VTK state from {path}")
     return ca.to_dict(int(n.value)), t.value, int(step.value), dt.value
+
+
+def write_trace(outdir: str, first_index: int, steps: list[dict]):
+    """Host-only writer of bbpgdtrace files in the reference's format."""
+    arr = (abi.TraceStep * max(len(steps), 1))()
+    for i, d in enumerate(steps):
+        for k, v in d.items():
+            setattr(arr[i], k, v)
+    rc = load_library().pcc_vtk_write_trace(str(outdir).encode(), int(first_index), arr, len(steps))
+    if rc != 0:
+        raise PccError(rc, "pcc_vtk_write_trace failed")

@@ -60,3 +60,37 @@ def test_restart_from_logged_state(tmp_path):
     h.set_clock(t, step)
     st = h.step()
     assert st["n_cells"] >= len(cells["x"]) and st["max_overlap"] <= p.tolerance
+
+
+def test_bbpgd_trace_matches_reference(tmp_path):
+    """-log_bbgd_trace: residual tested every iteration and one record per
+    iteration with the energy terms; the device records follow the
+    reference's within rounding of the (reordered) sums."""
+    from oracles import RefColony
+    from test_vtk import read_trace_dir
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx, log_bbpgd_trace=1)
+    ref = RefColony(p, outdir=str(tmp_path / "ref"))
+    ref.set_cells(sub(fx, "cells_"))
+    sr = ref.solve(p.dt, 0)
+    want = read_trace_dir(tmp_path / "ref" / "logs")
+    g = Colony(p)
+    g.set_trace_dir(str(tmp_path / "dev"))
+    g.set_cells(sub(fx, "cells_"))
+    sg = g.solve(p.dt, 0)
+    got = g.bbpgd_trace()
+    assert sg["relcp_iterations"] == sr["relcp_iterations"]
+    assert [r["step"] for r in got] == [r["step"] for r in want]
+    assert [r["recursive_iteration"] for r in got] == [r["recursive_iteration"] for r in want]
+    assert [r["total_constraints"] for r in got] == [r["total_constraints"] for r in want]
+    for k in ("residual", "step_size", "linear", "quadratic", "growth", "total"):
+        a = np.array([r[k] for r in got])
+        b = np.array([r[k] for r in want])  # 6 significant digits in the files
+        np.testing.assert_allclose(a, b, rtol=2e-5, atol=1e-12, err_msg=k)
+    # the same records are on disk in the trace directory
+    assert len(read_trace_dir(tmp_path / "dev")) == len(got)
+    # a step that is not a multiple of 10 is not traced
+    g2 = Colony(p)
+    g2.set_cells(sub(fx, "cells_"))
+    g2.solve(p.dt, 3)
+    assert g2.bbpgd_trace() == []

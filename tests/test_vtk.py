@@ -107,3 +107,41 @@ def test_empty_colony_and_ghost_copies_write(tmp_path, ref_logged):
     # which is small near both ends of the x axis
     near = (r >= 8.0) & (r * np.sin(np.radians(np.minimum(ang, 360 - ang))) < 2.5)
     assert f'NumberOfPoints="{int(near.sum())}"' in g
+
+
+def read_trace_dir(d: Path) -> list[dict]:
+    """The records of bbpgdtrace_<k> files (k = 1, 2, ...) from their field data."""
+    out = []
+    k = 1
+    while (d / f"bbpgdtrace_{k:07d}.pvtu").exists():
+        text = (d / "data" / f"bbpgdtrace_{k:07d}_rank_0000.vtu").read_text().splitlines()
+        rec = {}
+        for i, line in enumerate(text):
+            if "<DataArray" in line and "NumberOfTuples" in line:
+                name = line.split('Name="')[1].split('"')[0]
+                v = text[i + 1].strip()
+                rec[name] = int(v) if name in ("step", "recursive_iteration", "total_constraints") else float(v)
+        out.append(rec)
+        k += 1
+    return out
+
+
+@pytest.fixture(scope="module")
+def ref_trace(tmp_path_factory):
+    fx = load_fixture("hard_r10_seed3")
+    p = params_of(fx, log_bbpgd_trace=1)
+    ref = RefColony(p, outdir=str(tmp_path_factory.mktemp("reftrace")))
+    ref.set_cells(sub(fx, "cells_"))
+    st = ref.solve(p.dt, 0)
+    return p, Path(ref._tmp) / "logs", st
+
+
+def test_trace_files_byte_identical(ref_trace, tmp_path):
+    p, d, st = ref_trace
+    recs = read_trace_dir(d)
+    # one record per BBPGD iteration of every phase, residual tested every iteration
+    assert len(recs) == sum(1 for r in recs if r["step"] == 0) + st["bbpgd_iterations"]
+    device.write_trace(str(tmp_path), 1, recs)
+    for k in (1, len(recs) // 2, len(recs)):
+        _same(tmp_path / f"bbpgdtrace_{k:07d}.pvtu", d / f"bbpgdtrace_{k:07d}.pvtu")
+        _same(tmp_path / "data" / f"bbpgdtrace_{k:07d}_rank_0000.vtu", d / "data" / f"bbpgdtrace_{k:07d}_rank_0000.vtu")
