@@ -1172,7 +1172,9 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   if (coop == 0) {
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0))) return e;
-    coop = per_sm * ctx->num_sms;
+    // at most 4 blocks per SM: the two grid barriers of every iteration cost
+    // more with more arriving blocks than the extra resident warps hide
+    coop = (per_sm < 4 ? per_sm : 4) * ctx->num_sms;
   }
   long long want = (long long)grid_for((long long)n);
   if (nchunks > want) want = nchunks;
