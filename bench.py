@@ -48,8 +48,9 @@ ALGO_BYTES = {"fp64": (312.0, 288.0), "mixed": (192.0, 144.0)}
 
 
 def colony_params(**over) -> abi.Params:
-    return abi.default_params(dt=3e-4, fixed_dt=0, dt_cap=1e-3, mode=abi.MODE_HARD,
-                              ghost_mode=abi.GHOSTS_SINGLE_RANK, seed=0, **over)
+    kw = dict(dt=3e-4, fixed_dt=0, dt_cap=1e-3, mode=abi.MODE_HARD, ghost_mode=abi.GHOSTS_SINGLE_RANK, seed=0)
+    kw.update(over)
+    return abi.default_params(**kw)
 
 
 def make_colony(radius: float, seed: int) -> dict:
@@ -423,6 +424,58 @@ def run_frozen(args):
                       "frac_of_hbm": algo / (ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"]}), flush=True)
 
 
+def run_grow(args):
+    """Grows one colony from a single cell (orientation from the seed) to
+    --radius with the hard model, CFL-adaptive dt capped at 1e-3 -- the run the
+    reference's R = 260 figures come from -- and reports the whole run."""
+    import torch
+    from pcc_b200 import build, device
+    build.build()
+    torch.cuda.init()
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
+    p = colony_params(dt=1e-3, precision=prec, capacity_hint=int(4.5 * args.radius ** 2 * 1.2) + 64)
+    col = device.Colony(p)
+    col.set_cells(abi.seed_cell(args.job_seed))
+    stream = torch.cuda.ExternalStream(col.stream, device="cuda:0")
+    col.profiling(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    tlast = t0
+    steps = bb = 0
+    cells = 0.0
+    radius = 0.0
+    marks = []
+    e0.record(stream)
+    st = {}
+    while radius < args.radius and time.time() - t0 < args.grow_seconds:
+        st = col.step()
+        steps += 1
+        cells += st["n_cells"]
+        bb += st["bbpgd_iterations"]
+        radius = st["colony_radius"]
+        if not marks or radius >= marks[-1]["radius"] + 20.0:
+            marks.append({"radius": radius, "step": steps, "cells": st["n_cells"], "wall_s": time.time() - t0,
+                          "dt": st["dt_used"], "bbpgd_step": st["bbpgd_iterations"]})
+        if time.time() - tlast > 10:
+            tlast = time.time()
+            print(json.dumps({"step": steps, "radius": radius, "cells": st["n_cells"], "dt": st["dt_used"],
+                              "bbpgd": st["bbpgd_iterations"], "wall_s": tlast - t0}), file=sys.stderr, flush=True)
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.time() - t0
+    dev_ms = e0.elapsed_time(e1)
+    prof = col.profile()
+    final = col.get_cells()
+    print(json.dumps({
+        "grow": True, "precision": args.precision, "radius_target": args.radius, "radius": radius,
+        "reached": radius >= args.radius, "steps": steps, "cells": int(st.get("n_cells", 1)),
+        "cell_steps": cells, "wall_s": wall, "device_s": dev_ms / 1e3, "cell_steps_per_s": cells / (dev_ms / 1e3),
+        "bbpgd_iterations": bb, "bbpgd_iterations_per_s": bb / (dev_ms / 1e3),
+        "stage_ms": {"bbpgd": prof["bbpgd_ms"], "detect": prof["detect_ms"], "solve": prof["solve_ms"]},
+        "packing_fraction": packing_fraction(final), "sim_time": st.get("sim_time"), "marks": marks,
+    }), flush=True)
+
+
 def colony_jobs(n: int, rng, r_min: float, r_max: float, hard_frac: float, arrivals=None) -> list[dict]:
     """Colony jobs as in the batch sweep / serving configs: sequential seeds,
     growth rate g ~ U[0.5, 1.5] (tau = 1/g), R_end log-uniform in [r_min, r_max],
@@ -515,8 +568,12 @@ def main():
     ap.add_argument("--baseline-jobs", type=int, default=8)
     ap.add_argument("--job-seed", type=int, default=0)
     ap.add_argument("--max-bbpgd", type=int, default=500000, help="BBPGD iteration cap of each job")
+    ap.add_argument("--grow", action="store_true", help="grow one colony from a single cell to --radius")
+    ap.add_argument("--grow-seconds", type=float, default=1500.0, help="wall-clock limit of --grow")
     args = ap.parse_args()
-    if args.jobs > 0 or args.rate > 0:
+    if args.grow:
+        run_grow(args)
+    elif args.jobs > 0 or args.rate > 0:
         run_jobs(args)
     elif args.frozen:
         run_frozen(args)

@@ -102,7 +102,9 @@ typedef struct pcc_params {
   int solver_variant;                  /* PCC_SOLVER_AUTO or PCC_SOLVER_GENERAL */
   double log_every_colony_radius_delta;  /* VTK output cadence of the driver (CLI default 0.5) */
   double log_every_sim_time_delta;       /* ... and by simulated time (CLI default 100000) */
-  int log_bbpgd_trace;                   /* -log_bbgd_trace: trace BBPGD on every 10th step */
+  int log_bbpgd_trace;                   /* 1: -log_bbgd_trace, trace BBPGD on every 10th step;
+                                            2: record every solve without changing the solver
+                                            (residual still tested every 10th iteration) */
 } pcc_params;
 
 /* BBPGD kernel choice.  A planar colony (every z = 0, rotation about z only)

@@ -136,7 +136,7 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
   int phase = 0;
   // BBPGD trace on every 10th step (dynamics/models/Hard.cpp:107-111); a new
   // logger clears the earlier trace files
-  ctx->trace_active = ctx->params.log_bbpgd_trace && iter % 10 == 0;
+  ctx->trace_active = (ctx->params.log_bbpgd_trace == 1 && iter % 10 == 0) || ctx->params.log_bbpgd_trace == 2;
   if (ctx->trace_active) {
     ctx->trace_host.clear();
     vtk_clear_prefix(ctx->trace_dir, "bbpgdtrace");

@@ -47,7 +47,9 @@ struct SolverArgs {
   long long nchunks;
   SolverScalars* sc;
   DevStatus* st;
-  // BBPGD trace (-log_bbgd_trace): residual every iteration and the energy terms
+  // BBPGD trace (-log_bbgd_trace): residual every iteration and the energy
+  // terms; 1 tests convergence at every iteration as the reference does while
+  // tracing, 2 records without changing when convergence is tested
   int trace;
   double* tr_part;     // 2 per block (cell terms), then 1 per chunk (linear term)
   double* trace_out;   // kTraceWidth per iteration
@@ -429,7 +431,8 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
         int conv = 0;
         if (check) {
           sc->residual = v[3];
-          if (v[3] <= a.tol) conv = 1;
+          // a recording-only trace (trace == 2) keeps the every-10th test
+          if (v[3] <= a.tol && (a.trace != 2 || it % 10 == 0)) conv = 1;
         }
         if (!conv) {
           // BB1 on even, BB2 on odd iterations (BBPGD.cpp:98-112)
@@ -442,7 +445,13 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
             num = v[1];
           }
           if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
-          sc->alpha = dvd(num, den);
+          // Both BB quotients are >= 0 in exact arithmetic (the gradient is
+          // monotone); near convergence rounding can make the numerator a tiny
+          // negative number, and a negative step lifts an inactive constraint
+          // to gamma ~ 1e-26 > 0, where the projected residual counts its full
+          // positive gradient and never returns below tol.  Clamp at 0.
+          const double step = dvd(num, den);
+          sc->alpha = step > 0.0 ? step : 0.0;
         }
         sc->converged = conv;
         sc->iterations = it;
@@ -745,7 +754,8 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         int conv = 0;
         if (check) {
           sc->residual = v[3];
-          if (v[3] <= a.tol) conv = 1;
+          // a recording-only trace (trace == 2) keeps the every-10th test
+          if (v[3] <= a.tol && (a.trace != 2 || it % 10 == 0)) conv = 1;
         }
         if (!conv) {
           double num, den;
@@ -757,7 +767,13 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
             num = v[1];
           }
           if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
-          sc->alpha = dvd(num, den);
+          // Both BB quotients are >= 0 in exact arithmetic (the gradient is
+          // monotone); near convergence rounding can make the numerator a tiny
+          // negative number, and a negative step lifts an inactive constraint
+          // to gamma ~ 1e-26 > 0, where the projected residual counts its full
+          // positive gradient and never returns below tol.  Clamp at 0.
+          const double step = dvd(num, den);
+          sc->alpha = step > 0.0 ? step : 0.0;
         }
         sc->converged = conv;
         sc->iterations = it;
@@ -1075,7 +1091,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     // 2 per block of the largest grid, 1 per chunk
     if ((e = ctx->tr_part.reserve((size_t)(2 * 8 * ctx->num_sms * 8 + nchunks + 1), 0, s))) return e;
   }
-  a.trace = tracing ? 1 : 0;
+  a.trace = tracing ? (ctx->params.log_bbpgd_trace == 2 ? 2 : 1) : 0;
   a.tr_part = ctx->tr_part.p;
   a.trace_out = ctx->trace_dev.p;
   a.trace_cap = trace_cap;
