@@ -27,6 +27,8 @@ namespace {
 constexpr int kChunk = 1024;            // constraints per reduction chunk
 constexpr int kPerThread = kChunk / kBlock;
 constexpr long long kSpinLimit = 1LL << 26;
+constexpr int kSmallCells = 1024;        // one-block BBPGD up to this many cells ...
+constexpr int kSmallConstraints = 4096;  // ... and constraints
 
 struct SolverArgs {
   // constraints
@@ -79,6 +81,10 @@ __device__ __forceinline__ double vscale(double a, double x) {
 }
 
 __device__ __forceinline__ bool barrier(SolverScalars* sc, unsigned nblocks, DevStatus* st) {
+  if (nblocks == 1) {  // one block: a block barrier orders its global writes
+    __syncthreads();
+    return true;
+  }
   __shared__ unsigned s_gen;
   __shared__ int s_ok;
   __syncthreads();
@@ -111,6 +117,12 @@ __device__ __forceinline__ bool barrier(SolverScalars* sc, unsigned nblocks, Dev
 // Barrier whose last arriving block first runs `reduce` (all its threads).
 template <typename R>
 __device__ __forceinline__ bool barrier_reduce(SolverScalars* sc, unsigned nblocks, DevStatus* st, R reduce) {
+  if (nblocks == 1) {
+    __syncthreads();
+    reduce();
+    __syncthreads();
+    return true;
+  }
   __shared__ unsigned s_gen;
   __shared__ int s_last, s_ok;
   __syncthreads();
@@ -1195,10 +1207,17 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   long long want = (long long)grid_for((long long)n);
   if (nchunks > want) want = nchunks;
   if (want > coop) want = coop;
+  // Small colonies run in one block: its barriers are block barriers, it
+  // needs no co-residency guarantee, so it is an ordinary launch that runs
+  // beside other colonies' kernels.  The result does not depend on the grid.
+  if (n <= (size_t)kSmallCells && m <= (size_t)kSmallConstraints) want = 1;
   if (want < 1) want = 1;
   void* args[] = {mixed ? (void*)&pf : planar ? (void*)&pa : (void*)&a};
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], s);
-  e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)want), dim3(kBlock), args, 0, s);
+  if (want == 1)
+    e = cudaLaunchKernel(kern, dim3(1), dim3(kBlock), args, 0, s);
+  else
+    e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)want), dim3(kBlock), args, 0, s);
   ctx->launches++;
   if (e) return e;
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);
