@@ -327,7 +327,10 @@ __device__ __forceinline__ void trace_chunk(double* sm, double lin, double* tr_p
   if (threadIdx.x == 0) tr_part[2 * nb + ch] = v[0];
 }
 
+// kTr = 1 compiles the trace hooks in; the untraced kernel carries none of them.
+template <int kTr>
 __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
+  const int TR = kTr ? a.trace : 0;
   __shared__ double sm[4 * kBlock];
   const unsigned nb = gridDim.x;
   const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
@@ -338,8 +341,8 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   {
     double eq = 0.0, eg = 0.0;
     for (long long p = tid; p < a.n; p += stride)
-      cell_pass(a, p, 0, nullptr, nullptr, 0.0, false, a.trace ? &eq : nullptr, &eg);
-    if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+      cell_pass(a, p, 0, nullptr, nullptr, 0.0, false, TR ? &eq : nullptr, &eg);
+    if (TR) trace_cells(sm, eq, eg, a.tr_part);
   }
   if (!barrier(sc, nb, a.st)) return;
   for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
@@ -354,11 +357,11 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
       a.gam[0][c] = gm;
       double r = proj_grad_abs(g, gm);
       v[3] = v[3] < r ? r : v[3];
-      if (a.trace) lin = add(lin, mul(gm, a.phi[c]));
+      if (TR) lin = add(lin, mul(gm, a.phi[c]));
     }
     block_reduce4(v, sm);
     if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
-    if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
+    if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
   }
   auto reduce_init = [&]() {
     double v[4] = {0, 0, 0, 0};
@@ -373,7 +376,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
       sc->alpha = 1.0 / v[3];
       sc->converged = 0;
     }
-    if (a.trace)
+    if (TR)
       trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
                    a.trace_cap);
   };
@@ -384,7 +387,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   while (it < a.max_it) {
     const double alpha = *(volatile double*)&sc->alpha;
     // with the trace on the residual is evaluated (and tested) every iteration (BBPGD.cpp:73)
-    const bool check = (it % 10) == 0 || a.trace;
+    const bool check = (it % 10) == 0 || TR;
     const double* gp = a.gam[p];
     const double* gg = a.g[p];
     double* gc_out = a.gam[1 - p];
@@ -392,8 +395,8 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
     {
       double eq = 0.0, eg = 0.0;
       for (long long q = tid; q < a.n; q += stride)
-        cell_pass(a, q, 1, gp, gg, alpha, check, a.trace ? &eq : nullptr, &eg);
-      if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+        cell_pass(a, q, 1, gp, gg, alpha, check, TR ? &eq : nullptr, &eg);
+      if (TR) trace_cells(sm, eq, eg, a.tr_part);
     }
     if (!barrier(sc, nb, a.st)) return;
     for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
@@ -415,7 +418,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
           double r = proj_grad_abs(g, gam);
           v[3] = v[3] < r ? r : v[3];
         }
-        if (a.trace) lin = add(lin, mul(gam, a.phi[c]));
+        if (TR) lin = add(lin, mul(gam, a.phi[c]));
       }
       block_reduce4(v, sm);
       if (threadIdx.x == 0) {
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
         a.partials[4 * ch + 2] = v[2];
         a.partials[4 * ch + 3] = v[3];
       }
-      if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
+      if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
     }
     auto reduce_iter = [&]() {
       double v[4] = {0, 0, 0, 0};
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
         v[3] = v[3] < r ? r : v[3];
       }
       block_reduce4(v, sm);
-      if (a.trace)
+      if (TR)
         trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, it, v[3], alpha, a.trace_out,
                      a.trace_cap);
       if (threadIdx.x == 0) {
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
         if (check) {
           sc->residual = v[3];
           // a recording-only trace (trace == 2) keeps the every-10th test
-          if (v[3] <= a.tol && (a.trace != 2 || it % 10 == 0)) conv = 1;
+          if (v[3] <= a.tol && (TR != 2 || it % 10 == 0)) conv = 1;
         }
         if (!conv) {
           // BB1 on even, BB2 on odd iterations (BBPGD.cpp:98-112)
@@ -651,8 +654,9 @@ __device__ __forceinline__ double planar_grad(const PlanarArgs<Real>& a, long lo
   }
 }
 
-template <class Real>
+template <class Real, int kTr>
 __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
+  const int TR = kTr ? a.trace : 0;
   __shared__ double sm[4 * kBlock];
   const unsigned nb = gridDim.x;
   const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
@@ -662,8 +666,8 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
   {
     double eq = 0.0, eg = 0.0;
     for (long long p = tid; p < a.n; p += stride)
-      planar_cell_pass(a, p, 0, a.st[0], 0.0, false, a.trace ? &eq : nullptr, &eg);
-    if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+      planar_cell_pass(a, p, 0, a.st[0], 0.0, false, TR ? &eq : nullptr, &eg);
+    if (TR) trace_cells(sm, eq, eg, a.tr_part);
   }
   if (!barrier(sc, nb, a.st_err)) return;
   for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
@@ -678,12 +682,12 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         a.st[0][c].y = g;
         double r = proj_grad_abs(g, gm);
         v[3] = v[3] < r ? r : v[3];
-        if (a.trace) lin = add(lin, mul(gm, a.phi[c]));
+        if (TR) lin = add(lin, mul(gm, a.phi[c]));
       }
     }
     block_reduce4(v, sm);
     if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
-    if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
+    if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
   }
   auto reduce_init = [&]() {
     double v[4] = {0, 0, 0, 0};
@@ -698,7 +702,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
       sc->alpha = 1.0 / v[3];
       sc->converged = 0;
     }
-    if (a.trace)
+    if (TR)
       trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
                    a.trace_cap);
   };
@@ -708,14 +712,14 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
   long long it = 1;
   while (it < a.max_it) {
     const double alpha = *(volatile double*)&sc->alpha;
-    const bool check = (it % 10) == 0 || a.trace;
+    const bool check = (it % 10) == 0 || TR;
     const double4* sp = a.st[p];
     double4* so = a.st[1 - p];
     {
       double eq = 0.0, eg = 0.0;
       for (long long q = tid; q < a.n; q += stride)
-        planar_cell_pass(a, q, 1, sp, alpha, check, a.trace ? &eq : nullptr, &eg);
-      if (a.trace) trace_cells(sm, eq, eg, a.tr_part);
+        planar_cell_pass(a, q, 1, sp, alpha, check, TR ? &eq : nullptr, &eg);
+      if (TR) trace_cells(sm, eq, eg, a.tr_part);
     }
     if (!barrier(sc, nb, a.st_err)) return;
     for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
@@ -737,7 +741,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
             double r = proj_grad_abs(g, gam);
             v[3] = v[3] < r ? r : v[3];
           }
-          if (a.trace) lin = add(lin, mul(gam, a.phi[c]));
+          if (TR) lin = add(lin, mul(gam, a.phi[c]));
         }
       }
       block_reduce4(v, sm);
@@ -747,7 +751,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         a.partials[4 * ch + 2] = v[2];
         a.partials[4 * ch + 3] = v[3];
       }
-      if (a.trace) trace_chunk(sm, lin, a.tr_part, nb, ch);
+      if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
     }
     auto reduce_iter = [&]() {
       double v[4] = {0, 0, 0, 0};
@@ -759,7 +763,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         v[3] = v[3] < r ? r : v[3];
       }
       block_reduce4(v, sm);
-      if (a.trace)
+      if (TR)
         trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, it, v[3], alpha, a.trace_out,
                      a.trace_cap);
       if (threadIdx.x == 0) {
@@ -767,7 +771,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
         if (check) {
           sc->residual = v[3];
           // a recording-only trace (trace == 2) keeps the every-10th test
-          if (v[3] <= a.tol && (a.trace != 2 || it % 10 == 0)) conv = 1;
+          if (v[3] <= a.tol && (TR != 2 || it % 10 == 0)) conv = 1;
         }
         if (!conv) {
           double num, den;
@@ -1194,8 +1198,13 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     pf.cell = ctx->pf_cell.p;
     pf.u = ctx->pf_u.p;
   }
-  const void* kern = mixed ? (const void*)k_bbpgd_planar<float>
-                           : planar ? (const void*)k_bbpgd_planar<double> : (const void*)k_bbpgd;
+  const void* kern;
+  if (tracing)
+    kern = mixed ? (const void*)k_bbpgd_planar<float, 1>
+                 : planar ? (const void*)k_bbpgd_planar<double, 1> : (const void*)k_bbpgd<1>;
+  else
+    kern = mixed ? (const void*)k_bbpgd_planar<float, 0>
+                 : planar ? (const void*)k_bbpgd_planar<double, 0> : (const void*)k_bbpgd<0>;
   int& coop = mixed ? ctx->coop_blocks_mixed : planar ? ctx->coop_blocks_planar : ctx->coop_blocks;
   if (coop == 0) {
     int per_sm = 0;
