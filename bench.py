@@ -513,8 +513,11 @@ def run_jobs(args):
         jobs = colony_jobs(len(arr), rng, args.r_min, args.r_max, args.hard_frac, arr)
     else:
         jobs = colony_jobs(args.jobs, rng, args.r_min, args.r_max, args.hard_frac)
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
     for j in jobs:
         j["params"].max_bbpgd_iterations = args.max_bbpgd
+        if j["hard"]:
+            j["params"].precision = prec
     res, wall = device.serve(jobs, slots=args.slots, hbm_budget_bytes=args.hbm_budget, check=False)
     failed = [dict(job=k, status=abi.STATUS_NAMES.get(r["status"], r["status"]), steps=r["steps"], cells=r["cells"],
                    radius=r["radius"], dt=r["dt"], r_end=jobs[k]["end_radius"], hard=jobs[k]["hard"],
@@ -522,11 +525,22 @@ def run_jobs(args):
               for k, r in enumerate(res) if r["status"] != 0]
     lat = np.array([r["finish_s"] - r["arrival_s"] for r in res])
     cells = sum(r["cell_steps"] for r in res)
-    sample = [dict(j, arrival_s=0.0) for j in jobs[: args.baseline_jobs]]
+    # baseline: a sample of the same jobs one at a time on the plain FP64 path
+    sample = []
+    for j in jobs[: args.baseline_jobs]:
+        q = abi.Params.from_buffer_copy(j["params"])
+        q.precision = abi.PRECISION_FP64
+        sample.append(dict(j, params=q, arrival_s=0.0))
     res1, wall1 = device.serve(sample, slots=1, hbm_budget_bytes=args.hbm_budget, check=False)
-    same = all(a["checksum"] == b["checksum"] and a["steps"] == b["steps"] and a["status"] == b["status"]
-               for a, b in zip(res1, res))
     seq_rate = sum(r["cell_steps"] for r in res1) / wall1
+    # the same jobs alone with the mix's own settings: results must be identical
+    if prec == abi.PRECISION_FP64:
+        alone = res1
+    else:
+        alone, _ = device.serve([dict(j, arrival_s=0.0) for j in jobs[: min(2, args.baseline_jobs)]], slots=1,
+                                hbm_budget_bytes=args.hbm_budget, check=False)
+    same = all(a["checksum"] == b["checksum"] and a["steps"] == b["steps"] and a["status"] == b["status"]
+               for a, b in zip(alone, res))
     line = {
         "metric": METRIC, "mode": "serve" if args.rate > 0 else "batch",
         "jobs": len(jobs), "hard_jobs": sum(j["hard"] for j in jobs), "slots": args.slots,
@@ -534,13 +548,15 @@ def run_jobs(args):
         "colonies_per_s": len(jobs) / wall, "cell_steps_per_s": cells / wall, "wall_s": wall,
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "max": float(lat.max())},
-        "one_at_a_time": {"jobs": len(sample), "cell_steps_per_s": seq_rate, "wall_s": wall1},
+        "one_at_a_time": {"jobs": len(sample), "cell_steps_per_s": seq_rate, "wall_s": wall1,
+                          "path": "plain FP64, one job at a time (slots = 1)"},
         "speedup_vs_one_at_a_time": (cells / wall) / seq_rate,
         "results_identical_alone_and_in_mix": same,
         "max_step_bbpgd": int(max(r["max_step_bbpgd"] for r in res)),
         "failed_jobs": failed,
         "config": {"r_end": [args.r_min, args.r_max], "growth_rate": [0.5, 1.5], "hard_fraction": args.hard_frac,
-                   "hbm_budget_bytes": args.hbm_budget, "tolerance": 1e-3, "dtype": "f64"},
+                   "hbm_budget_bytes": args.hbm_budget, "tolerance": 1e-3,
+                   "dtype": "f64" if prec == abi.PRECISION_FP64 else "hard jobs mixed (f32 operands, f64 accumulation)"},
     }
     print(json.dumps(line), flush=True)
 

@@ -15,7 +15,7 @@
 //       [-l0 1] [-lambda 1e-2] [-kcc 2e4] [-tolerance 1e-3] [-max_bbpgd_iterations 5e5]
 //       [-max_recursive_iterations 50] [-linked_cell_size 2.2*l0] [-cfl_factor 0.5]
 //       [-log_every_colony_radius_delta 0.5] [-log_every_sim_time_delta 1e5]
-//       [-starter_vtk path] [-no_vtk] [-precision fp64|mixed]
+//       [-starter_vtk path] [-no_vtk] [-precision fp64|mixed] [-log_bbgd_trace]
 //       [-seed 0] [-fixed_dt 0|1] [-dt_cap 0] [-ghosts single_rank|none] [-max_steps N]
 //       [-device 0] [-out cells.csv]
 #include <dirent.h>
@@ -106,6 +106,11 @@ int main(int argc, char** argv) {
   p.log_every_sim_time_delta = o.num("-log_every_sim_time_delta", p.log_every_sim_time_delta);
   p.precision = strcasecmp(o.get("-precision", "fp64").c_str(), "mixed") == 0 ? PCC_PRECISION_MIXED
                                                                                : PCC_PRECISION_FP64;
+  // -log_bbgd_trace [true|1]: BBPGD trace of every 10th step into ./logs
+  if (o.has("-log_bbgd_trace")) {
+    const std::string v = o.get("-log_bbgd_trace", "");
+    p.log_bbpgd_trace = (v.empty() || v == "1" || strcasecmp(v.c_str(), "true") == 0) ? 1 : 0;
+  }
   const long long max_steps = (long long)o.num("-max_steps", 1e12);
   const int device = (int)o.num("-device", 0);
   const bool vtk = !o.has("-no_vtk");

@@ -94,3 +94,27 @@ def test_bbpgd_trace_matches_reference(tmp_path):
     g2.set_cells(sub(fx, "cells_"))
     g2.solve(p.dt, 3)
     assert g2.bbpgd_trace() == []
+
+
+def test_command_line_driver_logs_and_restarts(tmp_path):
+    """The C++ driver with the reference's options writes the reference's
+    output tree and restarts from it with -starter_vtk."""
+    import subprocess
+    from pathlib import Path
+    exe = Path(__file__).resolve().parents[1] / "proliferatingcellcollectives-idp_b200" / "pcc_cellcollectives"
+    run = subprocess.run([str(exe), "-mode", "hard", "-dt", "1e-3", "-fixed_dt", "1", "-end_radius", "2.5",
+                          "-seed", "3"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert run.returncode == 0, run.stderr
+    out = tmp_path / "vtk_output_hard"
+    assert (out / "parameters_0000000.pvtu").exists()
+    logs = sorted(out.glob("particles_*.pvtu"))
+    sims = sorted(out.glob("simulation_*.pvtu"))
+    assert len(logs) >= 3 and len(logs) == len(sims)
+    assert len(sorted((out / "data").glob("ghost_particles_*_rank_0000.vtu"))) == len(logs)
+    cells, t, step, dt = device.load_vtk(str(out))
+    assert len(cells["x"]) >= 2 and t > 0 and step > 0
+    again = subprocess.run([str(exe), "-mode", "hard", "-dt", "1e-3", "-fixed_dt", "1", "-end_radius", "3.0",
+                            "-starter_vtk", str(out)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert again.returncode == 0, again.stderr
+    assert f"Loading {len(cells['x'])} particles" in again.stdout
+    assert len(sorted(out.glob("particles_*.pvtu"))) > len(logs)
