@@ -105,20 +105,6 @@ __device__ __forceinline__ double4 ldcg<double4>(const double4* p) {
   return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
-// Loads of data that no thread writes while the kernel runs, through the
-// non-coherent read-only path: these lines stay cached in L1 across the grid
-// barriers of a persistent kernel, whose acquire fences drop coherent lines.
-template <typename T>
-__device__ __forceinline__ T ldro(const T* p) {
-  return __ldg(p);
-}
-template <>
-__device__ __forceinline__ double4 ldro<double4>(const double4* p) {
-  const double2 lo = __ldg(reinterpret_cast<const double2*>(p));
-  const double2 hi = __ldg(reinterpret_cast<const double2*>(p) + 1);
-  return make_double4(lo.x, lo.y, hi.x, hi.y);
-}
-
 __device__ __forceinline__ void raise_error(DevStatus* st, unsigned flag, int where) {
   atomicOr(&st->flags, flag);
   atomicExch(&st->where, where);

@@ -555,11 +555,11 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long
   Real f0 = 0, f1 = 0, f5 = 0;
   double g0 = 0, g1 = 0, g5 = 0;  // D^T gamma (trace only)
   double sg = 0.0;
-  const int b = ldro(a.inc_off + p), e = ldro(a.inc_off + p + 1);
+  const int b = a.inc_off[p], e = a.inc_off[p + 1];
 #pragma unroll 4
   for (int k = b; k < e; ++k) {
-    const long long c = ldro(a.inc_ent + k) >> 1;
-    const auto d = ldro(a.inc + k);
+    const long long c = a.inc_ent[k] >> 1;
+    const auto d = a.inc[k];
     const double4 s = ldcg(stp + c);
     const double gc = mode == 0 ? s.z : project(s.x, s.y, alpha);
     const double diff = sub(gc, s.z);
@@ -581,7 +581,7 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long
       g5 = add(g5, mul((double)d.z, gc));
     }
   }
-  const auto cl = ldro(a.cell + p);
+  const auto cl = a.cell[p];
   double ux, uy, wz;
   const double ldp = cl.w;
   if constexpr (kF64) {
@@ -624,10 +624,10 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long
 
 template <class Real>
 __device__ __forceinline__ double planar_grad(const PlanarArgs<Real>& a, long long c) {
-  const int2 ij = ldro(a.ij + c);
-  const auto n = ldro(a.nn + c);
-  const auto t = ldro(a.tt + c);
-  const auto s = ldro(a.ss + c);
+  const int2 ij = a.ij[c];
+  const auto n = a.nn[c];
+  const auto t = a.tt[c];
+  const auto s = a.ss[c];
   const auto ui = ldcg(a.u + ij.x);
   const auto uj = ldcg(a.u + ij.y);
   if constexpr (sizeof(Real) == 8) {
@@ -641,7 +641,7 @@ __device__ __forceinline__ double planar_grad(const PlanarArgs<Real>& a, long lo
     double gr = 0.0;
     gr = add(gr, mul(s.x, ui.w));
     gr = add(gr, mul(s.y, uj.w));
-    return add(ldro(a.phi + c), add(mul(a.dt, pd), mul(-a.dt, gr)));
+    return add(a.phi[c], add(mul(a.dt, pd), mul(-a.dt, gr)));
   } else {
     float pd = n.x * ui.x;
     pd = fmaf(n.y, ui.y, pd);
@@ -650,7 +650,7 @@ __device__ __forceinline__ double planar_grad(const PlanarArgs<Real>& a, long lo
     pd = fmaf(-n.y, uj.y, pd);
     pd = fmaf(t.y, uj.z, pd);
     const float gr = fmaf(s.y, uj.w, s.x * ui.w);
-    return ldro(a.phi + c) + a.dt * ((double)pd - (double)gr);
+    return a.phi[c] + a.dt * ((double)pd - (double)gr);
   }
 }
 
