@@ -355,6 +355,22 @@ pcc_status pcc_get_bbpgd_trace(const pcc_ctx* ctx, pcc_bbpgd_trace_step* out, si
 /* Sets the simulated time and the step counter of a context (after a restart). */
 pcc_status pcc_set_clock(pcc_ctx* ctx, double sim_time, long long iteration);
 
+/* Request loop (no counterpart in the reference): the admission and
+ * execution of pcc_serve as a long-lived server that accepts jobs while it
+ * runs.  submit queues a job (arrival = submit time; PCC_ERR_CAPACITY if its
+ * projected footprint alone exceeds the budget); a scheduler thread admits
+ * queued jobs in submit order as slots and budget free up; poll returns up to
+ * cap finished results with their ids, waiting up to wait_s seconds for the
+ * first; destroy finishes every queued and running job, then frees the
+ * server (results not polled by then are dropped). */
+typedef struct pcc_server pcc_server;
+pcc_status pcc_server_create(int slots, double hbm_budget_bytes, int device, pcc_server** out);
+pcc_status pcc_server_submit(pcc_server* server, const pcc_job* job, unsigned long long* id);
+pcc_status pcc_server_poll(pcc_server* server, pcc_job_result* out, unsigned long long* ids, size_t cap, size_t* n,
+                           double wait_s);
+pcc_status pcc_server_pending(pcc_server* server, size_t* queued, size_t* running);
+pcc_status pcc_server_destroy(pcc_server* server);
+
 /* The CUDA stream all work of the context is queued on (a cudaStream_t). */
 void* pcc_get_stream(const pcc_ctx* ctx);
 

@@ -17,7 +17,9 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -173,3 +175,129 @@ extern "C" pcc_status pcc_serve(const pcc_job* jobs, size_t n_jobs, int slots, d
     if (results[i].status != PCC_OK) return results[i].status;
   return PCC_OK;
 }
+
+// ----------------------------------------------------------------- request loop
+// The same admission and execution as pcc_serve, as a long-lived server that
+// takes jobs while it runs: pcc_server_submit queues a job (its arrival time
+// is the submit time), a scheduler thread admits queued jobs in submit order
+// as slots and HBM budget free up, each admitted job runs on its own context,
+// stream and thread, and pcc_server_poll hands back finished results.
+struct pcc_server {
+  int slots = 1;
+  double budget = 0;
+  int device = 0;
+  Clock::time_point t0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::pair<unsigned long long, pcc_job>> queue;
+  std::deque<std::pair<unsigned long long, pcc_job_result>> done;
+  std::vector<std::thread> workers;
+  std::thread scheduler;
+  int in_flight = 0;
+  double used = 0;
+  bool stop = false;
+  unsigned long long next_id = 1;
+};
+
+namespace {
+
+void server_loop(pcc_server* sv) {
+  std::unique_lock<std::mutex> lock(sv->mu);
+  for (;;) {
+    sv->cv.wait(lock, [&] {
+      if (sv->stop && sv->queue.empty()) return true;
+      if (sv->queue.empty()) return false;
+      const double need = projected_footprint(sv->queue.front().second.end_radius);
+      return sv->in_flight < sv->slots && sv->used + need <= sv->budget;
+    });
+    if (sv->queue.empty()) return;  // stopping with nothing queued
+    auto item = sv->queue.front();
+    sv->queue.pop_front();
+    const double need = projected_footprint(item.second.end_radius);
+    ++sv->in_flight;
+    sv->used += need;
+    sv->workers.emplace_back([sv, item, need] {
+      pcc_job_result r;
+      std::memset(&r, 0, sizeof r);
+      r.arrival_s = item.second.arrival_s;
+      r.footprint_bytes = need;
+      run_job(item.second, sv->device, sv->t0, &r);
+      std::lock_guard<std::mutex> g(sv->mu);
+      sv->done.emplace_back(item.first, r);
+      --sv->in_flight;
+      sv->used -= need;
+      sv->cv.notify_all();
+    });
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+pcc_status pcc_server_create(int slots, double hbm_budget_bytes, int device, pcc_server** out) {
+  if (!out || slots < 1 || !(hbm_budget_bytes > 0)) return PCC_ERR_INVALID;
+  auto* sv = new (std::nothrow) pcc_server();
+  if (!sv) return PCC_ERR_NOMEM;
+  sv->slots = slots;
+  sv->budget = hbm_budget_bytes;
+  sv->device = device;
+  sv->t0 = Clock::now();
+  sv->scheduler = std::thread(server_loop, sv);
+  *out = sv;
+  return PCC_OK;
+}
+
+pcc_status pcc_server_submit(pcc_server* sv, const pcc_job* job, unsigned long long* id) {
+  if (!sv || !job) return PCC_ERR_INVALID;
+  if (projected_footprint(job->end_radius) > sv->budget) return PCC_ERR_CAPACITY;
+  std::lock_guard<std::mutex> g(sv->mu);
+  if (sv->stop) return PCC_ERR_INVALID;
+  pcc_job j = *job;
+  j.arrival_s = std::chrono::duration<double>(Clock::now() - sv->t0).count();
+  const unsigned long long k = sv->next_id++;
+  sv->queue.emplace_back(k, j);
+  if (id) *id = k;
+  sv->cv.notify_all();
+  return PCC_OK;
+}
+
+pcc_status pcc_server_poll(pcc_server* sv, pcc_job_result* out, unsigned long long* ids, size_t cap, size_t* n,
+                           double wait_s) {
+  if (!sv || !n || (cap && (!out || !ids))) return PCC_ERR_INVALID;
+  std::unique_lock<std::mutex> lock(sv->mu);
+  if (sv->done.empty() && wait_s > 0)
+    sv->cv.wait_for(lock, std::chrono::duration<double>(wait_s), [&] { return !sv->done.empty(); });
+  size_t k = 0;
+  while (k < cap && !sv->done.empty()) {
+    ids[k] = sv->done.front().first;
+    out[k] = sv->done.front().second;
+    sv->done.pop_front();
+    ++k;
+  }
+  *n = k;
+  return PCC_OK;
+}
+
+pcc_status pcc_server_pending(pcc_server* sv, size_t* queued, size_t* running) {
+  if (!sv) return PCC_ERR_INVALID;
+  std::lock_guard<std::mutex> g(sv->mu);
+  if (queued) *queued = sv->queue.size();
+  if (running) *running = (size_t)sv->in_flight;
+  return PCC_OK;
+}
+
+pcc_status pcc_server_destroy(pcc_server* sv) {
+  if (!sv) return PCC_OK;
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv.notify_all();
+  if (sv->scheduler.joinable()) sv->scheduler.join();  // admits what was queued, then exits
+  for (auto& t : sv->workers) t.join();
+  delete sv;
+  return PCC_OK;
+}
+
+}  // extern "C"

@@ -52,6 +52,11 @@ def load_library(path: str | os.PathLike | None = None):
     lib.pcc_get_profile.argtypes = [VP, P(abi.Profile)]
     lib.pcc_serve.argtypes = [P(abi.Job), C.c_size_t, C.c_int, C.c_double, C.c_int, P(abi.JobResult),
                               P(C.c_double)]
+    lib.pcc_server_create.argtypes = [C.c_int, C.c_double, C.c_int, P(VP)]
+    lib.pcc_server_submit.argtypes = [VP, P(abi.Job), P(C.c_ulonglong)]
+    lib.pcc_server_poll.argtypes = [VP, P(abi.JobResult), P(C.c_ulonglong), C.c_size_t, P(C.c_size_t), C.c_double]
+    lib.pcc_server_pending.argtypes = [VP, P(C.c_size_t), P(C.c_size_t)]
+    lib.pcc_server_destroy.argtypes = [VP]
     lib.pcc_get_stream.restype = VP
     lib.pcc_get_stream.argtypes = [VP]
     lib.pcc_launch_count.restype = C.c_longlong
@@ -319,3 +324,52 @@ def write_trace(outdir: str, first_index: int, steps: list[dict]):
     rc = load_library().pcc_vtk_write_trace(str(outdir).encode(), int(first_index), arr, len(steps))
     if rc != 0:
         raise PccError(rc, "pcc_vtk_write_trace failed")
+
+
+class Server:
+    """A running request loop (pcc_server): submit colony jobs while it runs,
+    poll finished results by id."""
+
+    def __init__(self, slots: int, hbm_budget_bytes: float = 150e9, device: int = 0):
+        self.lib = load_library()
+        self.h = C.c_void_p()
+        rc = self.lib.pcc_server_create(int(slots), float(hbm_budget_bytes), device, C.byref(self.h))
+        if rc != 0:
+            raise PccError(rc, "pcc_server_create failed")
+
+    def submit(self, job: dict) -> int:
+        j = abi.Job()
+        j.params = job["params"]
+        j.end_radius = float(job["end_radius"])
+        j.arrival_s = 0.0
+        j.max_steps = int(job.get("max_steps", 0))
+        k = C.c_ulonglong(0)
+        rc = self.lib.pcc_server_submit(self.h, C.byref(j), C.byref(k))
+        if rc != 0:
+            raise PccError(rc, f"pcc_server_submit: {abi.STATUS_NAMES.get(rc, rc)}")
+        return int(k.value)
+
+    def poll(self, wait_s: float = 0.0, cap: int = 64) -> dict:
+        res = (abi.JobResult * cap)()
+        ids = (C.c_ulonglong * cap)()
+        n = C.c_size_t(0)
+        rc = self.lib.pcc_server_poll(self.h, res, ids, cap, C.byref(n), float(wait_s))
+        if rc != 0:
+            raise PccError(rc, "pcc_server_poll failed")
+        return {int(ids[i]): res[i].as_dict() for i in range(int(n.value))}
+
+    def pending(self) -> tuple[int, int]:
+        q, r = C.c_size_t(0), C.c_size_t(0)
+        self.lib.pcc_server_pending(self.h, C.byref(q), C.byref(r))
+        return int(q.value), int(r.value)
+
+    def close(self):
+        if self.h:
+            self.lib.pcc_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

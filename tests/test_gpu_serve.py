@@ -56,3 +56,29 @@ def test_admission_respects_slots_and_budget():
     # a job that can never fit is refused up front
     with pytest.raises(PccError):
         serve(jobs, slots=2, hbm_budget_bytes=one * 0.5)
+
+
+def test_request_loop_accepts_jobs_while_running():
+    """pcc_server: jobs submitted while others run are admitted as slots free
+    up, and each finishes exactly as it does alone."""
+    import time
+    from pcc_b200.device import Server
+    jobs = make_jobs()
+    alone, _ = serve(jobs, slots=1)
+    sv = Server(slots=3)
+    ids = []
+    for j in jobs:
+        ids.append(sv.submit(j))
+        time.sleep(0.05)
+    got = {}
+    deadline = time.time() + 600
+    while len(got) < len(jobs) and time.time() < deadline:
+        got.update(sv.poll(wait_s=1.0))
+    q, r = sv.pending()
+    sv.close()
+    assert (q, r) == (0, 0) and sorted(got) == sorted(ids)
+    for k, a in zip(ids, alone):
+        b = got[k]
+        for f in ("status", "steps", "cells", "bbpgd_iterations", "checksum"):
+            assert a[f] == b[f], (f, a, b)
+        assert b["arrival_s"] <= b["start_s"] <= b["finish_s"]
