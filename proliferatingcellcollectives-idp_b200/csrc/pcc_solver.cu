@@ -27,8 +27,10 @@ namespace {
 constexpr int kChunk = 1024;            // constraints per reduction chunk
 constexpr int kPerThread = kChunk / kBlock;
 constexpr long long kSpinLimit = 1LL << 26;
-constexpr int kSmallCells = 1024;        // one-block BBPGD up to this many cells ...
-constexpr int kSmallConstraints = 4096;  // ... and constraints
+constexpr int kSmallCells = 4096;         // planar: one 1024-thread CTA up to this many cells ...
+constexpr int kSmallConstraints = 16384;  // ... and constraints
+constexpr int kOneBlockCells = 1024;      // otherwise one 256-thread block up to this many cells ...
+constexpr int kOneBlockConstraints = 4096;  // ... and constraints
 
 struct SolverArgs {
   // constraints
@@ -808,6 +810,172 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
   }
 }
 
+// ------------------------------------------------------- one-CTA form, small colonies
+// A colony of up to kSmallCells cells and kSmallConstraints constraints runs
+// its whole BBPGD in one 1024-thread block: four 256-thread groups share the
+// work, each group reduces the chunks it owns with its own named barrier and
+// the same tree as block_reduce4, and group 0 reduces the chunk partials in
+// the same order as the multi-block kernel.  Every value is therefore the
+// multi-block kernel's, bit for bit; the iteration costs block barriers
+// instead of grid barriers and four times the threads of the one-block launch.
+constexpr int kSmallThreads = 4 * kBlock;
+constexpr int kSmallGroups = kSmallThreads / kBlock;
+
+__device__ __forceinline__ void group_sync(int grp) {
+  asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(kBlock) : "memory");
+}
+
+__device__ __forceinline__ void group_reduce4(double v[4], double* sm, int grp) {
+  const int t = threadIdx.x & (kBlock - 1);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) sm[q * kBlock + t] = v[q];
+  group_sync(grp);
+  for (int w = kBlock / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      sm[t] = add(sm[t], sm[t + w]);
+      sm[kBlock + t] = add(sm[kBlock + t], sm[kBlock + t + w]);
+      sm[2 * kBlock + t] = add(sm[2 * kBlock + t], sm[2 * kBlock + t + w]);
+      double x = sm[3 * kBlock + t], y = sm[3 * kBlock + t + w];
+      sm[3 * kBlock + t] = x < y ? y : x;
+    }
+    group_sync(grp);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = sm[q * kBlock];
+  group_sync(grp);
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kSmallThreads, 1) k_bbpgd_planar_small(PlanarArgs<Real> a) {
+  __shared__ double sm[kSmallGroups][4 * kBlock];
+  __shared__ double s_alpha;
+  __shared__ int s_conv;
+  const int grp = threadIdx.x / kBlock, lane = threadIdx.x % kBlock;
+  SolverScalars* sc = a.sc;
+
+  for (long long p = threadIdx.x; p < a.n; p += kSmallThreads) planar_cell_pass(a, p, 0, a.st[0], 0.0, false);
+  __syncthreads();
+  for (long long ch = grp; ch < a.nchunks; ch += kSmallGroups) {
+    double v[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < kPerThread; ++k) {
+      const long long c = ch * kChunk + k * kBlock + lane;
+      if (c < a.m) {
+        const double g = planar_grad(a, c);
+        const double gm = a.st[0][c].x;
+        a.st[0][c].y = g;
+        double r = proj_grad_abs(g, gm);
+        v[3] = v[3] < r ? r : v[3];
+      }
+    }
+    group_reduce4(v, sm[grp], grp);
+    if (lane == 0) a.partials[4 * ch + 3] = v[3];
+  }
+  __syncthreads();
+  if (grp == 0) {
+    double v[4] = {0, 0, 0, 0};
+    for (long long ch = lane; ch < a.nchunks; ch += kBlock) {
+      double r = ldcg(a.partials + 4 * ch + 3);
+      v[3] = v[3] < r ? r : v[3];
+    }
+    group_reduce4(v, sm[0], 0);
+    if (lane == 0) {
+      sc->res0 = v[3];
+      sc->residual = v[3];
+      s_alpha = 1.0 / v[3];
+      s_conv = 0;
+    }
+  }
+  __syncthreads();
+
+  int p = 0;
+  long long it = 1;
+  while (it < a.max_it) {
+    const double alpha = s_alpha;
+    const bool check = (it % 10) == 0;
+    const double4* sp = a.st[p];
+    double4* so = a.st[1 - p];
+    for (long long q = threadIdx.x; q < a.n; q += kSmallThreads) planar_cell_pass(a, q, 1, sp, alpha, check);
+    __syncthreads();
+    for (long long ch = grp; ch < a.nchunks; ch += kSmallGroups) {
+      double v[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int k = 0; k < kPerThread; ++k) {
+        const long long c = ch * kChunk + k * kBlock + lane;
+        if (c < a.m) {
+          const double4 s = ldcg(sp + c);
+          const double gam = project(s.x, s.y, alpha);
+          const double g = planar_grad(a, c);
+          so[c] = make_double4(gam, g, s.z, 0.0);
+          const double dgm = sub(gam, s.x), dg = sub(g, s.y);
+          v[0] = add(v[0], mul(dgm, dgm));
+          v[1] = add(v[1], mul(dgm, dg));
+          v[2] = add(v[2], mul(dg, dg));
+          if (check) {
+            double r = proj_grad_abs(g, gam);
+            v[3] = v[3] < r ? r : v[3];
+          }
+        }
+      }
+      group_reduce4(v, sm[grp], grp);
+      if (lane == 0) {
+        a.partials[4 * ch + 0] = v[0];
+        a.partials[4 * ch + 1] = v[1];
+        a.partials[4 * ch + 2] = v[2];
+        a.partials[4 * ch + 3] = v[3];
+      }
+    }
+    __syncthreads();
+    if (grp == 0) {
+      double v[4] = {0, 0, 0, 0};
+      for (long long ch = lane; ch < a.nchunks; ch += kBlock) {
+        v[0] = add(v[0], ldcg(a.partials + 4 * ch + 0));
+        v[1] = add(v[1], ldcg(a.partials + 4 * ch + 1));
+        v[2] = add(v[2], ldcg(a.partials + 4 * ch + 2));
+        double r = ldcg(a.partials + 4 * ch + 3);
+        v[3] = v[3] < r ? r : v[3];
+      }
+      group_reduce4(v, sm[0], 0);
+      if (lane == 0) {
+        int conv = 0;
+        if (check) {
+          sc->residual = v[3];
+          if (v[3] <= a.tol) conv = 1;
+        }
+        if (!conv) {
+          double num, den;
+          if (it % 2 == 0) {
+            num = v[0];
+            den = v[1];
+          } else {
+            den = v[2];
+            num = v[1];
+          }
+          if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
+          const double step = dvd(num, den);  // clamped at 0 as in k_bbpgd_planar
+          s_alpha = step > 0.0 ? step : 0.0;
+        }
+        s_conv = conv;
+        sc->iterations = it;
+      }
+    }
+    __syncthreads();
+    if (s_conv) break;
+    p = 1 - p;
+    ++it;
+  }
+  if (threadIdx.x == 0) {
+    sc->iterations = it;
+    sc->converged = s_conv;
+    sc->alpha = s_alpha;
+  }
+  if (!s_conv) return;
+  for (long long c = threadIdx.x; c < a.m; c += kSmallThreads) {
+    a.gamma[c] = ldcg(a.st[p] + c).x;
+    a.phi[c] = ldcg(a.st[1 - p] + c).y;
+  }
+}
+
 // Packs the planar operands of one ReLCP phase.
 template <class V2>
 __device__ __forceinline__ V2 mk2(double a, double b);
@@ -1198,15 +1366,19 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     pf.cell = ctx->pf_cell.p;
     pf.u = ctx->pf_u.p;
   }
+  // small planar colonies without a trace: the one-CTA kernel (same values)
+  const bool small = planar && !tracing && n <= (size_t)kSmallCells && m <= (size_t)kSmallConstraints;
   const void* kern;
-  if (tracing)
+  if (small)
+    kern = mixed ? (const void*)k_bbpgd_planar_small<float> : (const void*)k_bbpgd_planar_small<double>;
+  else if (tracing)
     kern = mixed ? (const void*)k_bbpgd_planar<float, 1>
                  : planar ? (const void*)k_bbpgd_planar<double, 1> : (const void*)k_bbpgd<1>;
   else
     kern = mixed ? (const void*)k_bbpgd_planar<float, 0>
                  : planar ? (const void*)k_bbpgd_planar<double, 0> : (const void*)k_bbpgd<0>;
   int& coop = mixed ? ctx->coop_blocks_mixed : planar ? ctx->coop_blocks_planar : ctx->coop_blocks;
-  if (coop == 0) {
+  if (coop == 0 && !small) {
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0))) return e;
     // at most 4 blocks per SM: the two grid barriers of every iteration cost
@@ -1219,11 +1391,13 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   // Small colonies run in one block: its barriers are block barriers, it
   // needs no co-residency guarantee, so it is an ordinary launch that runs
   // beside other colonies' kernels.  The result does not depend on the grid.
-  if (n <= (size_t)kSmallCells && m <= (size_t)kSmallConstraints) want = 1;
+  if (n <= (size_t)kOneBlockCells && m <= (size_t)kOneBlockConstraints) want = 1;
   if (want < 1) want = 1;
   void* args[] = {mixed ? (void*)&pf : planar ? (void*)&pa : (void*)&a};
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], s);
-  if (want == 1)
+  if (small)
+    e = cudaLaunchKernel(kern, dim3(1), dim3(kSmallThreads), args, 0, s);
+  else if (want == 1)
     e = cudaLaunchKernel(kern, dim3(1), dim3(kBlock), args, 0, s);
   else
     e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)want), dim3(kBlock), args, 0, s);

@@ -320,3 +320,24 @@ def test_mixed_precision_trajectory_matches_reference():
     for k in range(int(want[0]) + 1, int(want[-1]) + 1):
         assert abs(int(np.argmax(got >= k)) - int(np.argmax(want >= k))) <= 50, k
     assert all(h["max_overlap"] <= p.tolerance for h in hist)
+
+
+def test_one_cta_solver_bit_identical_to_multi_block():
+    """A planar colony of ~2,900 cells solves in the one-CTA kernel (four
+    256-thread groups, block barriers); the 3D kernel runs the same solve over
+    a grid of blocks with grid barriers.  Same chunks, same reduction trees:
+    the results agree bit for bit."""
+    from pcc_b200 import synth
+    cells = synth.dense_colony(30.0, seed=1, lane_gap=0.0, end_gap=0.0)
+    out = []
+    for variant in (abi.SOLVER_AUTO, abi.SOLVER_GENERAL):
+        p = abi.default_params(dt=3e-4, fixed_dt=1, solver_variant=variant)
+        g = Colony(p)
+        g.set_cells(cells)
+        st = g.solve(p.dt, 1)
+        out.append((st, g.get_cells(), g.constraints()))
+    assert 1024 < len(cells["x"]) <= 4096 and out[0][0]["n_constraints"] > 4096
+    assert out[0][0] == out[1][0]
+    for k in ("x", "y", "q0", "q3", "length", "ldot", "stress", "force", "velocity"):
+        np.testing.assert_array_equal(out[0][1][k], out[1][1][k], err_msg=k)
+    np.testing.assert_array_equal(out[0][2]["gamma"], out[1][2]["gamma"])
