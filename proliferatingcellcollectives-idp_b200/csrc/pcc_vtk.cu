@@ -738,10 +738,18 @@ pcc_status pcc_log_vtk(pcc_ctx* ctx, const char* outdir, unsigned long long inde
     cudaMemcpyAsync(hd, d, nd * sizeof(double), cudaMemcpyDeviceToHost, ctx->vtk_stream);
     cudaMemcpyAsync(hi, ctx->vtk_idev.p, 2 * n * sizeof(int), cudaMemcpyDeviceToHost, ctx->vtk_stream);
   }
-  cudaEvent_t done;
-  if ((e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming))) return PCC_ERR_CUDA;
-  cudaEventRecord(done, ctx->vtk_stream);
-  if ((e = cudaGetLastError())) return PCC_ERR_CUDA;
+  cudaEvent_t done = nullptr;
+  e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+  if (!e) e = cudaEventRecord(done, ctx->vtk_stream);
+  if (!e) e = cudaGetLastError();
+  if (e) {
+    cudaStreamSynchronize(ctx->vtk_stream);  // no copy may still target the staging buffers
+    if (done) cudaEventDestroy(done);
+    if (hd) cudaFreeHost(hd);
+    if (hi) cudaFreeHost(hi);
+    ctx->err = std::string("pcc_log_vtk: ") + cudaGetErrorString(e);
+    return PCC_ERR_CUDA;
+  }
   const std::string dir(outdir);
   const bool with_rec = rec != nullptr;
   const pcc_sim_record r = rec ? *rec : pcc_sim_record{};
