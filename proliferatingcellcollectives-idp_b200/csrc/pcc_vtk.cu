@@ -669,14 +669,14 @@ pcc_status pcc_vtk_write_parameters(const char* outdir, unsigned long long index
   if (!outdir || !p) return PCC_ERR_INVALID;
   // ParameterLogger::log (logger/ParameterLogger.cpp:11-40); the three
   // settings the device path has no use for carry the reference CLI defaults
-  // (util/CLIParser.h:165-195): min_box_size (2, 2, 0), growth_factor 1.5,
-  // particle_preallocation_factor 20.
+  // (util/CLIParser.h:165-195): growth_factor 1.5, particle_preallocation_factor
+  // 20; min_box_size is (l0 + 1, l0 + 1, 0) as the parser sets it (233-236).
   std::vector<Field> f = {fd("dt_s", p->dt),
                           fd("end_radius", p->end_radius),
                           fd("log_every_colony_radius_delta", p->log_every_colony_radius_delta),
                           fd("log_every_sim_time_delta", p->log_every_sim_time_delta),
-                          fd("min_box_size_x", 2.0),
-                          fd("min_box_size_y", 2.0),
+                          fd("min_box_size_x", p->l0 + 1.0),
+                          fd("min_box_size_y", p->l0 + 1.0),
                           fd("min_box_size_z", 0.0),
                           fd("xi", p->xi),
                           fd("TAU", p->tau),

@@ -68,15 +68,63 @@ Options parse(int argc, char** argv) {
 
 }  // namespace
 
+// The options and their defaults (the reference's -help, util/CLIParser.h:13-160,
+// plus this driver's own switches).
+static void print_help(const pcc_params& p) {
+  auto row = [](const char* name, const char* what, const std::string& def) {
+    std::printf("  %-32s %-52s [default: %s]\n", name, what, def.c_str());
+  };
+  auto num = [](double v) {
+    char b[32];
+    std::snprintf(b, sizeof b, "%g", v);
+    return std::string(b);
+  };
+  std::printf("\nAvailable parameters:\n\nSimulation:\n");
+  row("-mode hard|soft", "Collision model (required)", "none");
+  row("-dt", "Time step", num(p.dt));
+  row("-end_radius", "Colony radius at which the run stops", num(p.end_radius));
+  row("-log_every_colony_radius_delta", "Log after the radius grew by this much (0: off)",
+      num(p.log_every_colony_radius_delta));
+  row("-log_every_sim_time_delta", "Log after this much simulated time (0: off)", num(p.log_every_sim_time_delta));
+  row("-cfl_factor", "CFL factor of the adaptive time step", num(p.cfl_factor));
+  row("-log_bbgd_trace", "Write a BBPGD trace on every 10th step to ./logs", "false");
+  row("-starter_vtk", "Restart from a VTK output directory or file", "none");
+  std::printf("\nPhysics:\n");
+  row("-xi", "Drag coefficient", num(p.xi));
+  row("-tau", "Growth time constant", num(p.tau));
+  row("-l0", "Reference length", num(p.l0));
+  row("-lambda", "Stress sensitivity of growth", num(p.lambda));
+  row("-kcc", "Soft-model contact stiffness", num(p.kcc));
+  std::printf("\nSolver:\n");
+  row("-tolerance", "BBPGD residual and ReLCP overlap tolerance", num(p.tolerance));
+  row("-max_bbpgd_iterations", "BBPGD iteration cap", num((double)p.max_bbpgd_iterations));
+  row("-max_recursive_iterations", "ReLCP phase cap", num((double)p.max_recursive_iterations));
+  row("-linked_cell_size", "Broadphase bin edge", "2.2 * l0");
+  std::printf("\nThis driver:\n");
+  row("-precision fp64|mixed", "BBPGD operand precision", "fp64");
+  row("-seed", "Seed of the first cell's orientation and the divisions", "0");
+  row("-fixed_dt 0|1", "Keep dt fixed instead of adapting it", "0");
+  row("-dt_cap", "Upper bound of the adapted dt (0: none)", "0");
+  row("-ghosts single_rank|none", "Self-ghost copies of the one-rank decomposition", "single_rank");
+  row("-max_steps", "Step cap", "none");
+  row("-device", "CUDA device", "0");
+  row("-no_vtk", "Write no VTK output", "false");
+  row("-out", "Write the final cells as CSV", "none");
+}
+
 int main(int argc, char** argv) {
   Options o = parse(argc, argv);
-  std::string mode = o.get("-mode", "");
-  if (mode.empty()) {
-    std::fprintf(stderr, "Error: Required parameter -mode not provided. Use -help for usage information.\n");
-    return 1;
-  }
   pcc_params p;
   pcc_default_params(&p);
+  if (o.has("-help")) {
+    print_help(p);
+    return 0;
+  }
+  std::string mode = o.get("-mode", "");
+  if (mode.empty()) {
+    std::printf("Error: Required parameter -mode not provided. Use -help for usage information.\n");
+    return 1;
+  }
   if (strcasecmp(mode.c_str(), "soft") == 0)
     p.mode = PCC_MODE_SOFT;
   else if (strcasecmp(mode.c_str(), "hard") == 0)
