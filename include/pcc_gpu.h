@@ -371,6 +371,19 @@ pcc_status pcc_server_poll(pcc_server* server, pcc_job_result* out, unsigned lon
 pcc_status pcc_server_pending(pcc_server* server, size_t* queued, size_t* running);
 pcc_status pcc_server_destroy(pcc_server* server);
 
+/* Lockstep batch of colonies (no counterpart in the reference): one context
+ * per colony, made from per_colony[k]; pcc_batch_step advances every colony
+ * by one pcc_step, spread over a pool of host threads so their kernels overlap
+ * on the device, and returns when all are done (out, if given, receives n
+ * stats; the first failing colony's status is returned).  pcc_batch_context
+ * gives colony k's context for upload, download and queries.  Each colony
+ * follows the trajectory it has alone. */
+typedef struct pcc_batch pcc_batch;
+pcc_status pcc_batch_create(const pcc_params* per_colony, int n, int device, pcc_batch** out);
+pcc_status pcc_batch_context(pcc_batch* batch, int k, pcc_ctx** ctx);
+pcc_status pcc_batch_step(pcc_batch* batch, pcc_step_stats* out);
+pcc_status pcc_batch_destroy(pcc_batch* batch);
+
 /* The CUDA stream all work of the context is queued on (a cudaStream_t). */
 void* pcc_get_stream(const pcc_ctx* ctx);
 

@@ -301,3 +301,106 @@ pcc_status pcc_server_destroy(pcc_server* sv) {
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------- lockstep batch
+// Many colonies stepped together: each colony is a context with its own
+// stream; pcc_batch_step advances every colony by one step, the colonies
+// spread over a pool of host threads so their kernels overlap on the device,
+// and returns when all are done.  A colony's trajectory is the one it has
+// alone (contexts share nothing).
+struct pcc_batch {
+  std::vector<pcc_ctx*> ctx;
+  std::vector<std::thread> pool;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  size_t next = 0, finished = 0, total = 0;
+  unsigned long long epoch = 0;
+  bool stop = false;
+  pcc_step_stats* out = nullptr;
+  std::vector<pcc_status> rc;
+};
+
+namespace {
+
+void batch_worker(pcc_batch* b) {
+  unsigned long long seen = 0;
+  std::unique_lock<std::mutex> lock(b->mu);
+  for (;;) {
+    b->cv_work.wait(lock, [&] { return b->stop || (b->epoch != seen && b->next < b->total); });
+    if (b->stop) return;
+    const size_t k = b->next++;
+    if (b->next >= b->total) seen = b->epoch;
+    lock.unlock();
+    pcc_step_stats st;
+    std::memset(&st, 0, sizeof st);
+    const pcc_status r = pcc_step(b->ctx[k], &st);
+    lock.lock();
+    b->rc[k] = r;
+    if (b->out) b->out[k] = st;
+    if (++b->finished == b->total) b->cv_done.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+pcc_status pcc_batch_create(const pcc_params* per_colony, int n, int device, pcc_batch** out) {
+  if (!per_colony || n < 1 || !out) return PCC_ERR_INVALID;
+  *out = nullptr;
+  auto* b = new (std::nothrow) pcc_batch();
+  if (!b) return PCC_ERR_NOMEM;
+  for (int k = 0; k < n; ++k) {
+    pcc_ctx* c = nullptr;
+    const pcc_status r = pcc_create(&per_colony[k], device, &c);
+    if (r != PCC_OK) {
+      for (auto* x : b->ctx) pcc_destroy(x);
+      delete b;
+      return r;
+    }
+    b->ctx.push_back(c);
+  }
+  b->rc.assign((size_t)n, PCC_OK);
+  const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+  const int workers = std::min<int>(n, (int)std::min(64u, 2 * hw));
+  for (int w = 0; w < workers; ++w) b->pool.emplace_back(batch_worker, b);
+  *out = b;
+  return PCC_OK;
+}
+
+pcc_status pcc_batch_context(pcc_batch* b, int k, pcc_ctx** ctx) {
+  if (!b || !ctx || k < 0 || (size_t)k >= b->ctx.size()) return PCC_ERR_INVALID;
+  *ctx = b->ctx[(size_t)k];
+  return PCC_OK;
+}
+
+pcc_status pcc_batch_step(pcc_batch* b, pcc_step_stats* out) {
+  if (!b) return PCC_ERR_INVALID;
+  std::unique_lock<std::mutex> lock(b->mu);
+  b->out = out;
+  b->total = b->ctx.size();
+  b->next = 0;
+  b->finished = 0;
+  ++b->epoch;
+  b->cv_work.notify_all();
+  b->cv_done.wait(lock, [&] { return b->finished == b->total; });
+  b->out = nullptr;
+  for (const pcc_status r : b->rc)
+    if (r != PCC_OK) return r;
+  return PCC_OK;
+}
+
+pcc_status pcc_batch_destroy(pcc_batch* b) {
+  if (!b) return PCC_OK;
+  {
+    std::lock_guard<std::mutex> g(b->mu);
+    b->stop = true;
+  }
+  b->cv_work.notify_all();
+  for (auto& t : b->pool) t.join();
+  for (auto* c : b->ctx) pcc_destroy(c);
+  delete b;
+  return PCC_OK;
+}
+
+}  // extern "C"

@@ -57,6 +57,10 @@ def load_library(path: str | os.PathLike | None = None):
     lib.pcc_server_poll.argtypes = [VP, P(abi.JobResult), P(C.c_ulonglong), C.c_size_t, P(C.c_size_t), C.c_double]
     lib.pcc_server_pending.argtypes = [VP, P(C.c_size_t), P(C.c_size_t)]
     lib.pcc_server_destroy.argtypes = [VP]
+    lib.pcc_batch_create.argtypes = [P(abi.Params), C.c_int, C.c_int, P(VP)]
+    lib.pcc_batch_context.argtypes = [VP, C.c_int, P(VP)]
+    lib.pcc_batch_step.argtypes = [VP, P(abi.StepStats)]
+    lib.pcc_batch_destroy.argtypes = [VP]
     lib.pcc_get_stream.restype = VP
     lib.pcc_get_stream.argtypes = [VP]
     lib.pcc_launch_count.restype = C.c_longlong
@@ -366,6 +370,59 @@ class Server:
     def close(self):
         if self.h:
             self.lib.pcc_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _BorrowedColony(Colony):
+    """A colony whose context belongs to a Batch (not destroyed here)."""
+
+    def __init__(self, lib, handle):  # noqa: D107 - no pcc_create
+        self.lib = lib
+        self.h = handle
+
+    def close(self):
+        self.h = C.c_void_p()
+
+
+class Batch:
+    """Colonies stepped together (pcc_batch): batch.step() advances every
+    colony once; batch[k] is colony k (upload, download, queries)."""
+
+    def __init__(self, params: list, device: int = 0):
+        self.lib = load_library()
+        arr = (abi.Params * len(params))(*params)
+        self.h = C.c_void_p()
+        rc = self.lib.pcc_batch_create(arr, len(params), device, C.byref(self.h))
+        if rc != 0:
+            raise PccError(rc, "pcc_batch_create failed")
+        self.n = len(params)
+        self._cols = []
+        for k in range(self.n):
+            c = C.c_void_p()
+            self.lib.pcc_batch_context(self.h, k, C.byref(c))
+            self._cols.append(_BorrowedColony(self.lib, c))
+
+    def __getitem__(self, k: int) -> Colony:
+        return self._cols[k]
+
+    def step(self) -> list[dict]:
+        st = (abi.StepStats * self.n)()
+        rc = self.lib.pcc_batch_step(self.h, st)
+        if rc != 0:
+            raise PccError(rc, _REFERENCE_MESSAGES.get(rc, f"pcc_batch_step: {abi.STATUS_NAMES.get(rc, rc)}"))
+        return [st[k].as_dict() for k in range(self.n)]
+
+    def close(self):
+        if self.h:
+            for c in self._cols:
+                c.close()
+            self.lib.pcc_batch_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

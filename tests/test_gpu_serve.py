@@ -82,3 +82,28 @@ def test_request_loop_accepts_jobs_while_running():
         for f in ("status", "steps", "cells", "bbpgd_iterations", "checksum"):
             assert a[f] == b[f], (f, a, b)
         assert b["arrival_s"] <= b["start_s"] <= b["finish_s"]
+
+
+def test_batch_steps_every_colony_as_alone():
+    """pcc_batch: four colonies stepped together (one context and stream each,
+    a host thread pool) end exactly where each ends when stepped alone."""
+    import numpy as np
+    from pcc_b200.device import Batch, Colony
+    # fixed dt: every colony has divided by step 1,000 (l grows by dt / tau per step)
+    params = [abi.default_params(dt=1e-3, fixed_dt=1, seed=200 + k, tau=1.0 / (0.7 + 0.2 * k)) for k in range(4)]
+    b = Batch(params)
+    for k in range(4):
+        b[k].set_cells(abi.seed_cell(200 + k))
+    for _ in range(1500):
+        stats = b.step()
+    got = [b[k].get_cells() for k in range(4)]
+    assert all(s["n_cells"] > 1 for s in stats)
+    for k in range(4):
+        g = Colony(params[k])
+        g.set_cells(abi.seed_cell(200 + k))
+        for _ in range(1500):
+            g.step()
+        want = g.get_cells()
+        for f in ("x", "y", "q0", "q3", "length"):
+            np.testing.assert_array_equal(got[k][f], want[f], err_msg=f)
+    b.close()
