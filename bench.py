@@ -338,11 +338,15 @@ def run_ours(args):
     if errors is not None:
         line["mixed_vs_fp64"] = errors
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, kind, k, ncpu, el = cpu_rate(True)
+        # one step of the same colony (~20 s of CPU work at R = 260): the first
+        # step from the packing, FP64, the reference's own code at release flags
+        rate, kind, k, ncpu, el = cpu_rate(True, seconds=0.0, radius=args.radius, min_steps=1, max_steps=1,
+                                           warmup=0)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
-                                "sample": f"{k} steps ({el:.1f} s) of the synthetic dense colony at "
-                                          f"R={CPU_SAMPLE_RADIUS:g} ({ncpu} cells); smaller colonies need "
-                                          f"fewer BBPGD iterations per cell, so this favours the CPU"}
+                                "sample": f"{k} step ({el:.1f} s) of the same synthetic dense colony at "
+                                          f"R={args.radius:g} ({ncpu} cells), the first step from the packing, "
+                                          f"FP64; one rank, one thread (the reference has no threaded path "
+                                          f"and no MPI is available)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     col.close()
