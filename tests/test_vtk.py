@@ -145,3 +145,18 @@ def test_trace_files_byte_identical(ref_trace, tmp_path):
     for k in (1, len(recs) // 2, len(recs)):
         _same(tmp_path / f"bbpgdtrace_{k:07d}.pvtu", d / f"bbpgdtrace_{k:07d}.pvtu")
         _same(tmp_path / "data" / f"bbpgdtrace_{k:07d}_rank_0000.vtu", d / "data" / f"bbpgdtrace_{k:07d}_rank_0000.vtu")
+
+
+def test_restart_reads_field_values_as_the_reference_does(tmp_path, ref_logged):
+    """VTKStateLoader reads a field value as the first run of digits, '.' and
+    '-' on its line, so an exponent is dropped ("3e-05" -> 3); the restart
+    loader keeps that reading."""
+    p, ref, cells = ref_logged
+    rec = dict(RECORD, dt_s=3e-05, simulation_time_s=2.5e-06, step=7)
+    device.write_particles(str(tmp_path), "particles", 7, cells)
+    device.write_simulation(str(tmp_path), 7, rec)
+    got = device.load_vtk(str(tmp_path))
+    want = ref_load_vtk(str(tmp_path))
+    assert got[1:] == want[1:] == (2.5, 7, 3.0)
+    for k in ("x", "y", "q0", "q3", "length", "force", "velocity"):
+        np.testing.assert_array_equal(got[0][k], want[0][k], err_msg=k)
