@@ -14,9 +14,14 @@
 //
 // Limits and sharing: at most kNoallocMaxCells cells and kNoallocMaxContacts
 // contacts per call (larger calls return PCC_ERR_CAPACITY before touching the
-// GPU).  Every call on a device uses the same scratch array, which keeps the
-// previous call's contents; the counters that must start at zero are cleared
-// on the caller's stream at the start of each call.  Calls that overlap on the
+// GPU).  Every gid_i / gid_j must be a cell index in [0, n): a contact with an
+// id outside that range is skipped on the device (no scratch or output entry
+// is touched for it), a flag in the scratch records it, and the call returns
+// PCC_ERR_BOUNDS.  To read that flag the call waits for its own work on
+// `stream` before it returns.  Every call on a device uses the same scratch
+// array, which keeps the previous call's contents; the counters and the flag
+// that must start at zero are cleared on the caller's stream at the start of
+// each call.  Calls that overlap on the
 // GPU (two streams, or two host threads) race on the scratch and must not be
 // issued concurrently on one device.
 //
@@ -24,7 +29,10 @@
 // array with cudaGetSymbolAddress while that device is current (the host-side
 // name of a __device__ array is only a stand-in and must never be passed to a
 // kernel); later calls reuse the cached address.  Make the first call on a
-// device before any stream capture on it.
+// device before any stream capture on it.  With lazy module loading (the
+// CUDA 12 default) that first call, and the first launch of each kernel here,
+// may also make the driver load this file's device code, which takes device
+// memory of the driver's own; warm calls allocate nothing.
 #include <cstdio>
 #include <mutex>
 
@@ -42,11 +50,13 @@ constexpr int kNoallocMaxDevices = 64;
 //   cursor    kNoallocMaxCells + 1 ints        fill cursors      (cleared per call)
 //   off       kNoallocMaxCells + 1 ints        incidence offsets
 //   ent       2 kNoallocMaxContacts ints       incidence entries (2c + side)
+//   flag      1 unsigned                       out-of-range contact seen (cleared per call)
 constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 constexpr size_t kFelBytes = align256(sizeof(double) * kNoallocMaxContacts);
 constexpr size_t kCellIntBytes = align256(sizeof(int) * (kNoallocMaxCells + 1));
 constexpr size_t kEntBytes = align256(sizeof(int) * 2 * kNoallocMaxContacts);
-constexpr size_t kScratchBytes = kFelBytes + 3 * kCellIntBytes + kEntBytes;  // 6.75 MiB
+constexpr size_t kFlagBytes = 256;
+constexpr size_t kScratchBytes = kFelBytes + 3 * kCellIntBytes + kEntBytes + kFlagBytes;  // 6.75 MiB
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -62,12 +72,22 @@ __device__ __forceinline__ double pow15_na(double x) {
   return p + (pe + x * ds);
 }
 
+// A contact whose ids are not both cell indices in [0, n) is left out.
+__device__ __forceinline__ bool na_ids_ok(int a, int b, long long n) {
+  return (unsigned)a < (unsigned long long)n && (unsigned)b < (unsigned long long)n;
+}
+
 __global__ void k_na_fel(const int* __restrict__ gi, const int* __restrict__ gj, const double* __restrict__ sd,
-                         long long m, const double* __restrict__ diam, double kcc, double* __restrict__ fel,
-                         int* __restrict__ cnt) {
+                         long long m, long long n, const double* __restrict__ diam, double kcc,
+                         double* __restrict__ fel, int* __restrict__ cnt, unsigned* __restrict__ flag) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m) return;
   const int a = gi[c], b = gj[c];
+  if (!na_ids_ok(a, b, n)) {
+    fel[c] = 0.0;
+    atomicOr(flag, 1u);
+    return;
+  }
   atomicAdd(&cnt[a], 1);
   atomicAdd(&cnt[b], 1);
   const double overlap = -sd[c];
@@ -103,11 +123,12 @@ __global__ void k_na_scan(const int* __restrict__ cnt, long long n, int* __restr
   }
 }
 
-__global__ void k_na_fill(const int* __restrict__ gi, const int* __restrict__ gj, long long m,
+__global__ void k_na_fill(const int* __restrict__ gi, const int* __restrict__ gj, long long m, long long n,
                           const int* __restrict__ off, int* __restrict__ cursor, int* __restrict__ ent) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m) return;
   const int a = gi[c], b = gj[c];
+  if (!na_ids_ok(a, b, n)) return;
   ent[off[a] + atomicAdd(&cursor[a], 1)] = (int)(2 * c);
   ent[off[b] + atomicAdd(&cursor[b], 1)] = (int)(2 * c + 1);
 }
@@ -173,6 +194,9 @@ extern "C" pcc_status pcc_soft_forces_noalloc(const int* gid_i, const int* gid_j
   if (!diameter || !force || !stress || (m && (!gid_i || !gid_j || !sd || !normal || !r_i || !r_j || !stress_i ||
                                                !stress_j)))
     return PCC_ERR_INVALID;
+  // an error left pending by earlier work in the process is not this call's:
+  // report it without launching (and without clearing it)
+  if (cudaPeekAtLastError() != cudaSuccess) return PCC_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) return PCC_ERR_CUDA;
   void* base = nullptr;
@@ -195,16 +219,32 @@ extern "C" pcc_status pcc_soft_forces_noalloc(const int* gid_i, const int* gid_j
   int* cursor = reinterpret_cast<int*>(b + kFelBytes + kCellIntBytes);
   int* off = reinterpret_cast<int*>(b + kFelBytes + 2 * kCellIntBytes);
   int* ent = reinterpret_cast<int*>(b + kFelBytes + 3 * kCellIntBytes);
+  unsigned* flag = reinterpret_cast<unsigned*>(b + kFelBytes + 3 * kCellIntBytes + kEntBytes);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // counters from the previous call must start at zero
+  // counters and the bounds flag from the previous call must start at zero
   if (cudaMemsetAsync(cnt, 0, sizeof(int) * (n + 1), s) != cudaSuccess ||
-      cudaMemsetAsync(cursor, 0, sizeof(int) * (n + 1), s) != cudaSuccess)
+      cudaMemsetAsync(cursor, 0, sizeof(int) * (n + 1), s) != cudaSuccess ||
+      cudaMemsetAsync(flag, 0, sizeof(unsigned), s) != cudaSuccess)
     return PCC_ERR_CUDA;
   const int T = pcc::kBlock;
-  if (m) k_na_fel<<<pcc::grid_for((long long)m, T), T, 0, s>>>(gid_i, gid_j, sd, (long long)m, diameter, kcc, fel, cnt);
+  if (m) {
+    k_na_fel<<<pcc::grid_for((long long)m, T), T, 0, s>>>(gid_i, gid_j, sd, (long long)m, (long long)n, diameter, kcc,
+                                                          fel, cnt, flag);
+    if (cudaGetLastError() != cudaSuccess) return PCC_ERR_CUDA;
+  }
   k_na_scan<<<1, 1024, 0, s>>>(cnt, (long long)n, off);
-  if (m) k_na_fill<<<pcc::grid_for((long long)m, T), T, 0, s>>>(gid_i, gid_j, (long long)m, off, cursor, ent);
+  if (cudaGetLastError() != cudaSuccess) return PCC_ERR_CUDA;
+  if (m) {
+    k_na_fill<<<pcc::grid_for((long long)m, T), T, 0, s>>>(gid_i, gid_j, (long long)m, (long long)n, off, cursor,
+                                                           ent);
+    if (cudaGetLastError() != cudaSuccess) return PCC_ERR_CUDA;
+  }
   k_na_gather<<<pcc::grid_for((long long)n, T), T, 0, s>>>((long long)n, off, ent, sd, normal, r_i, r_j, stress_i,
                                                            stress_j, fel, force, stress);
-  return cudaGetLastError() == cudaSuccess ? PCC_OK : PCC_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return PCC_ERR_CUDA;
+  unsigned host_flag = 0;
+  if (cudaMemcpyAsync(&host_flag, flag, sizeof host_flag, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return PCC_ERR_CUDA;
+  return host_flag ? PCC_ERR_BOUNDS : PCC_OK;
 }
