@@ -81,7 +81,7 @@ typedef struct pcc_params {
   double tau;         /* -tau: growth time constant */
   double l0;          /* -l0: birth length; cells divide at 2*l0 */
   double lambda;      /* -lambda: stress sensitivity of growth */
-  double temperature; /* -temperature: must be 0 here (Brownian kicks are not on the device path) */
+  double temperature; /* -temperature: Brownian rotational kicks (Physics.cpp:59-81); 0 turns them off */
   double kcc;         /* -kcc: Hertz constant of the soft model */
   int monolayer;      /* -monolayer (only affects Brownian kicks) */
   /* SolverConfig */
@@ -166,11 +166,16 @@ typedef struct pcc_profile {
   double cell_solves;           /* sum of cell counts over solves */
   long long detect_full_passes; /* detections that rebinned the colony (counted with profiling off too) */
   long long detect_list_passes; /* later ReLCP phases served from the candidate lists */
+  long long bbpgd_grid_launches;  /* BBPGD launches of the multi-block (grid-synchronised) kernel
+                                     (counted with profiling off too) */
+  long long bbpgd_cta_launches;   /* BBPGD launches of the one-block kernels (small colonies) */
 } pcc_profile;
 
 typedef struct pcc_ctx pcc_ctx;
 
-/* Reference defaults (CLIParser.h:296-365): hard mode, temperature 0, ghost
+/* Reference defaults (CLIParser.h:296-365), except temperature 0 (the
+ * reference's 1e-28 moves no quaternion at FP64 resolution and would cost a
+ * host draw per step): hard mode, ghost
  * copies as the reference driver makes them at one rank (PCC_GHOSTS_SINGLE_RANK). */
 void pcc_default_params(pcc_params* p);
 
@@ -225,10 +230,16 @@ pcc_status pcc_soft_forces_frozen(pcc_ctx* ctx, int repeats, float* ms_per_assem
  * (6 per cell: force, torque) and stress (1 per cell) are outputs, equal to
  * the force assembly of pcc_soft_forces_frozen / solveSoftPotential
  * (Soft.cpp:46-83).  Limit: 65536 cells and 393216 contacts per call
- * (PCC_ERR_CAPACITY beyond, before any GPU work).  Intermediates live in one
- * fixed 6.75 MiB device array that every call on a GPU shares, so calls must
- * not overlap on one device; the first call on a device looks the array up
- * and should come before any stream capture.  stream is a cudaStream_t
+ * (PCC_ERR_CAPACITY beyond, before any GPU work).  Every gid_i / gid_j must be
+ * a cell index in [0, n); a contact outside that range is skipped on the
+ * device and the call returns PCC_ERR_BOUNDS (the call waits for its own work
+ * on `stream` to read that flag back).  An error already pending from earlier
+ * work in the process makes the call return PCC_ERR_CUDA without launching.
+ * Intermediates live in one fixed 6.75 MiB device array that every call on a
+ * GPU shares, so calls must not overlap on one device; the first call on a
+ * device looks the array up and should come before any stream capture, and
+ * with lazy module loading it may make the driver load this code into device
+ * memory of its own (later calls allocate nothing).  stream is a cudaStream_t
  * (NULL: the default stream). */
 pcc_status pcc_soft_forces_noalloc(const int* gid_i, const int* gid_j, const double* sd, const double* normal,
                                    const double* r_i, const double* r_j, const double* stress_i,

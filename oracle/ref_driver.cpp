@@ -83,6 +83,11 @@ extern "C" double pcc_ref_division_length(unsigned long long seed, unsigned long
   return dis(gen);
 }
 
+// The reference's process-wide Brownian generator (dynamics/Physics.cpp:19).
+// A colony handle reseeds it with the default seed when it is created, so each
+// handle draws the stream a fresh reference process would.
+extern std::mt19937 gen;
+
 // ------------------------------------------------------------ colony handle
 namespace {
 struct RefColony {
@@ -137,6 +142,7 @@ extern "C" {
 
 void* pcc_ref_create(const pcc_params* p, const char* outdir) {
   auto* c = new RefColony();
+  gen.seed(std::mt19937::default_seed);
   fill_params(c->params, p);
   c->ghost_mode = p->ghost_mode;
   c->fixed_dt = p->fixed_dt;

@@ -112,6 +112,8 @@ class Profile(C.Structure):
         ("cell_solves", C.c_double),
         ("detect_full_passes", C.c_longlong),
         ("detect_list_passes", C.c_longlong),
+        ("bbpgd_grid_launches", C.c_longlong),
+        ("bbpgd_cta_launches", C.c_longlong),
     ]
 
     def as_dict(self) -> dict:

@@ -49,12 +49,33 @@ def build_cli(verbose: bool = False) -> Path:
     return CLI
 
 
+OBJ_DIR = PKG / "_build"
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles every source to an object in parallel (no device code crosses
+    files), then links the shared library."""
     if not force and not needs_build():
         build_cli(verbose)
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, f"-I{ROOT / 'include'}", f"-I{PKG / 'csrc'}", "-o", str(OUT) + ".tmp",
-           *[str(PKG / "csrc" / s) for s in SOURCES]]
+    from concurrent.futures import ThreadPoolExecutor
+
+    OBJ_DIR.mkdir(exist_ok=True)
+    inc = [f"-I{ROOT / 'include'}", f"-I{PKG / 'csrc'}"]
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src: str) -> Path:
+        obj = OBJ_DIR / (Path(src).stem + ".o")
+        cmd = [nvcc(), *compile_flags, *inc, "-c", "-o", str(obj), str(PKG / "csrc" / src)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(OUT) + ".tmp",
+           *[str(o) for o in objs]]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

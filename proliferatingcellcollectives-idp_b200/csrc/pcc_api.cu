@@ -146,6 +146,8 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
   ctx->ncons = 0;
   CU(reset_ldot(ctx), "reset");
   CU(mobility(ctx), "mobility");
+  // U_ext: Brownian kicks at ReLCP phase 0 only (Hard.cpp:138-143, Physics.cpp:68)
+  CU(brownian_draw(ctx), "brownian");
   while ((long long)phase < ctx->params.max_recursive_iterations) {
     const size_t before = ctx->ncons;
     double ov_old = 0.0, ov_new = 0.0;
@@ -164,6 +166,7 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
     int status = 0;
     ctx->trace_phase = phase;
     CU(bbpgd_solve(ctx, dt, &it, &res, &status), "bbpgd");
+    ctx->uext_active = false;
     total_it += it;
     if (status == PCC_ERR_NOCONV_BBPGD) return fail(ctx, status, "BBPGD did not converge");
     if (status) {
@@ -199,6 +202,7 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
 pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
   ctx->ncons = 0;
   CU(reset_ldot(ctx), "reset");
+  CU(brownian_draw(ctx), "brownian");  // Soft.cpp:94
   size_t added = 0;
   double max_ov = 0.0;
   if (ctx->profiling) cudaEventRecord(ctx->ev[2], ctx->stream);
@@ -206,6 +210,7 @@ pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
   CU(build_incidence(ctx), "incidence");
   profile_detect(ctx);
   CU(soft_forces_and_move(ctx, dt), "soft");
+  ctx->uext_active = false;
   CU(grow_cells(ctx, dt), "grow");
   pcc_status rc = check_device(ctx, "soft step");
   if (rc) return rc;
@@ -281,7 +286,7 @@ void pcc_default_params(pcc_params* p) {
 pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out) {
   if (!params || !out) return PCC_ERR_INVALID;
   *out = nullptr;
-  if (params->temperature > 0) return PCC_ERR_INVALID;  // Brownian kicks are not on the device path
+  if (!(params->temperature >= 0)) return PCC_ERR_INVALID;
   if (params->mode != PCC_MODE_HARD && params->mode != PCC_MODE_SOFT) return PCC_ERR_INVALID;
   if (params->precision != PCC_PRECISION_FP64 && params->precision != PCC_PRECISION_MIXED) return PCC_ERR_INVALID;
   if (!(params->linked_cell_size > 0) || !(params->xi > 0) || !(params->tau > 0)) return PCC_ERR_INVALID;
@@ -330,6 +335,7 @@ pcc_status pcc_destroy(pcc_ctx* ctx) {
   if (ctx->status) cudaFreeAsync(ctx->status, ctx->stream);
   if (ctx->status_host) cudaFreeHost(ctx->status_host);
   if (ctx->pinned_ll) cudaFreeHost(ctx->pinned_ll);
+  if (ctx->brown_host) cudaFreeHost(ctx->brown_host);
   cudaStream_t s = ctx->stream;
   delete ctx;  // device buffers are freed on the context's stream
   if (s) {

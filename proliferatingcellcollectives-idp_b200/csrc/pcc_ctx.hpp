@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -125,6 +126,16 @@ struct pcc_ctx {
   pcc::DevBuf<float2> pf_n, pf_t, pf_s;
   pcc::DevBuf<float4> pf_inc, pf_cell, pf_u;
   bool planar = false;  // set by the last binning pass
+
+  // Brownian external velocity (Physics.cpp:59-81, Particle.cpp:174-190): the
+  // reference draws it from one process-wide std::mt19937 with the default
+  // seed (Physics.cpp:19); each context holds that generator for its colony.
+  std::mt19937 brown_gen;
+  pcc::DevBuf<double> uext;             // 3 per cell: rotational U_ext (x, y, z)
+  pcc::DevBuf<double> brown_coef;       // 3 per cell: T u1 u_k of this draw
+  double* brown_host = nullptr;         // pinned staging of brown_coef
+  size_t brown_host_cap = 0;
+  bool uext_active = false;             // U_ext is non-zero in the current solve
 
   // step scratch
   pcc::DevBuf<int> div_flag, div_off;

@@ -26,6 +26,9 @@ cudaError_t detect_contacts(pcc_ctx* ctx, double tol, int phase, bool reuse, siz
 cudaError_t build_incidence(pcc_ctx* ctx);
 
 // ---- pcc_solver.cu
+// Draws the Brownian U_ext of every cell (temperature > 0) from the context's
+// generator and sets ctx->uext_active; a no-op at temperature 0.
+cudaError_t brownian_draw(pcc_ctx* ctx);
 // One BBPGD solve on the current constraint set (hard model).
 cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* residual, int* status);
 // Moves cells with the solver's velocities and writes back gamma / phi.

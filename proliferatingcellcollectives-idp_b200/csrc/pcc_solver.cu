@@ -47,6 +47,7 @@ struct SolverArgs {
   long long n;
   const int *inc_off, *inc_ent;
   const double *Mlin, *Mrot, *len, *ldot_prev;
+  const double* uext;  // rotational U_ext, 3 per cell (Brownian kicks at ReLCP phase 0); null: zero
   double *U, *dl, *F, *sig, *ldot, *imp;
   double dt, lambda, tau, tol;
   long long max_it;
@@ -210,7 +211,8 @@ __device__ __forceinline__ void cell_pass(const SolverArgs& a, long long p, int 
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     const double uc = add(0.0, mul(q < 3 ? ml : mr, F[q]));
-    U[q] = add(uc, 0.0);  // + U_ext (zero: no Brownian kicks)
+    // U = U_ext + M F (VecWAXPY, HardModelGradient.cpp:21); U_ext is rotational only
+    U[q] = add(uc, (q >= 3 && a.uext) ? a.uext[3 * p + q - 3] : 0.0);
   }
   double im = exp(vscale(-a.lambda, sg));
   double ld = vscale(dvd(1.0, a.tau), mul(a.len[p], im));
@@ -538,6 +540,7 @@ struct PlanarArgs {
   double4* st[2];
   const int *inc_off, *inc_ent;
   const V4 *inc, *cell;
+  const double* uext;  // rotational U_ext, 3 per cell (only z is used: monolayer kicks); null: zero
   V4* u;
   double *U, *F, *sig, *ldot, *imp;  // general-layout outputs on residual iterations
   double dt, lambda, tau, tol;
@@ -589,14 +592,15 @@ __device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long
   const auto cl = a.cell[p];
   double ux, uy, wz;
   const double ldp = cl.w;
+  const double uez = a.uext ? a.uext[3 * p + 2] : 0.0;
   if constexpr (kF64) {
     ux = add(add(0.0, mul(cl.x, f0)), 0.0);
     uy = add(add(0.0, mul(cl.x, f1)), 0.0);
-    wz = add(add(0.0, mul(cl.y, f5)), 0.0);
+    wz = add(add(0.0, mul(cl.y, f5)), uez);
   } else {
     ux = cl.x * f0;
     uy = cl.x * f1;
-    wz = cl.y * f5;
+    wz = (double)(cl.y * f5) + uez;
   }
   const double im = exp(vscale(-a.lambda, sg));
   const double ld = vscale(dvd(1.0, a.tau), mul((double)cl.z, im));
@@ -1110,7 +1114,7 @@ __global__ void k_soft_fel(ConsView cs, long long m, const double* __restrict__ 
 // stream for that cell), then U = M F, dC = G U and the move, growth rate.
 __global__ void k_soft_cell(CellsView c, long long n, ConsView cs, const int* __restrict__ inc_off,
                             const int* __restrict__ inc_ent, const double* __restrict__ fel, double xi, double lambda,
-                            double tau, double dt, int move) {
+                            double tau, double dt, int move, const double* __restrict__ uext) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double F[6] = {0, 0, 0, 0, 0, 0};
@@ -1152,7 +1156,9 @@ __global__ void k_soft_cell(CellsView c, long long n, ConsView cs, const int* __
   const double ml = dvd(1.0, mul(l, xi));
   const double mr = dvd(12.0, mul(mul(mul(l, l), l), xi));
   double u[6];
-  for (int d = 0; d < 6; ++d) u[d] = add(add(0.0, mul(d < 3 ? ml : mr, F[d])), 0.0);
+  // U = U_ext + M F (Soft.cpp:14-15); U_ext is rotational only
+  for (int d = 0; d < 6; ++d)
+    u[d] = add(add(0.0, mul(d < 3 ? ml : mr, F[d])), (d >= 3 && uext) ? uext[3 * i + d - 3] : 0.0);
   const double s = c.q0[i], wx = c.q1[i], wy = c.q2[i], wz = c.q3[i];
   double dC[7];
   for (int k = 0; k < 3; ++k) dC[k] = add(0.0, mul(1.0, u[k]));
@@ -1194,7 +1200,69 @@ __global__ void k_mobility(const double* __restrict__ len, long long n, double x
   Mr[i] = dvd(12.0, mul(mul(mul(l, l), l), xi));
 }
 
+// U_ext of one draw (Particle::calculateBrownianVelocity, Particle.cpp:174-190):
+// coef = T u1 u_k from the host, times the impedance three times in the
+// reference's left-to-right order, added into a zeroed vector (VecSetValues
+// ADD_VALUES, Physics.cpp:73-75).  Monolayer kicks have only the z component.
+__global__ void k_uext(const double* __restrict__ coef, const double* __restrict__ imp, long long n, int monolayer,
+                       double* __restrict__ uext) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double im = imp[i];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double v = (monolayer && k < 2) ? 0.0 : mul(mul(mul(coef[3 * i + k], im), im), im);
+    uext[3 * i + k] = add(0.0, v);
+  }
+}
+
 }  // namespace
+
+cudaError_t brownian_draw(pcc_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  const size_t n = ctx->n;
+  ctx->uext_active = false;
+  if (!(ctx->params.temperature > 0) || n == 0) return cudaSuccess;
+  cudaError_t e;
+  if ((e = ctx->uext.reserve(3 * n + 3, 0, s)) || (e = ctx->brown_coef.reserve(3 * n + 3, 0, s))) return e;
+  if (ctx->brown_host_cap < 3 * n) {
+    if (ctx->brown_host) {
+      if ((e = cudaStreamSynchronize(s))) return e;  // the last upload may still read it
+      cudaFreeHost(ctx->brown_host);
+      ctx->brown_host = nullptr;
+      ctx->brown_host_cap = 0;
+    }
+    const size_t cap = 3 * n + 3 * n / 2 + 192;
+    if ((e = cudaMallocHost(&ctx->brown_host, cap * sizeof(double)))) return e;
+    ctx->brown_host_cap = cap;
+  } else {
+    if ((e = cudaStreamSynchronize(s))) return e;  // the staging buffer is reused
+  }
+  // one uniform_real_distribution(-1, 1) per call, as Particle::calculateBrownianVelocity;
+  // the draw order is the particle order, i.e. global-id order after the x-sort
+  const double T = ctx->params.temperature;
+  const bool mono = ctx->params.monolayer != 0;
+  double* h = ctx->brown_host;
+  for (size_t i = 0; i < n; ++i) {
+    std::uniform_real_distribution<double> dist(-1.0, 1.0);
+    const double rot = T * dist(ctx->brown_gen);
+    if (mono) {
+      h[3 * i] = 0.0;
+      h[3 * i + 1] = 0.0;
+      h[3 * i + 2] = rot * dist(ctx->brown_gen);
+    } else {
+      h[3 * i] = rot * dist(ctx->brown_gen);
+      h[3 * i + 1] = rot * dist(ctx->brown_gen);
+      h[3 * i + 2] = rot * dist(ctx->brown_gen);
+    }
+  }
+  if ((e = cudaMemcpyAsync(ctx->brown_coef.p, h, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s))) return e;
+  k_uext<<<grid_for((long long)n), kBlock, 0, s>>>(ctx->brown_coef.p, ctx->cells.imp.p, (long long)n, mono ? 1 : 0,
+                                                   ctx->uext.p);
+  ctx->launches++;
+  ctx->uext_active = true;
+  return cudaGetLastError();
+}
 
 cudaError_t mobility(pcc_ctx* ctx) {
   cudaStream_t s = ctx->stream;
@@ -1254,6 +1322,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   a.Mrot = ctx->Mrot.p;
   a.len = ctx->cells.len.p;
   a.ldot_prev = ctx->cells.ldot.p;
+  a.uext = ctx->uext_active ? ctx->uext.p : nullptr;
   a.U = ctx->U.p;
   a.dl = ctx->dldot.p;
   a.F = ctx->F.p;
@@ -1283,7 +1352,9 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   a.trace_out = ctx->trace_dev.p;
   a.trace_cap = trace_cap;
 
-  const bool planar = ctx->planar && ctx->params.solver_variant != PCC_SOLVER_GENERAL;
+  // out-of-plane Brownian kicks (-monolayer off) leave the planar form
+  const bool planar = ctx->planar && ctx->params.solver_variant != PCC_SOLVER_GENERAL &&
+                      !(ctx->uext_active && !ctx->params.monolayer);
   const bool mixed = planar && ctx->params.precision == PCC_PRECISION_MIXED;
   PlanarArgs<double> pa;
   PlanarArgs<float> pf;
@@ -1335,6 +1406,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
       q.st[1] = ctx->p_st1.p;
       q.inc_off = ctx->inc_off.p;
       q.inc_ent = ctx->inc_ent.p;
+      q.uext = a.uext;
       q.U = ctx->U.p;
       q.F = ctx->F.p;
       q.sig = ctx->sig.p;
@@ -1404,6 +1476,10 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     e = cudaLaunchKernel(kern, dim3(1), dim3(kBlock), args, 0, s);
   else
     e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)want), dim3(kBlock), args, 0, s);
+  if (small || want == 1)
+    ctx->prof.bbpgd_cta_launches++;
+  else
+    ctx->prof.bbpgd_grid_launches++;
   ctx->launches++;
   if (e) return e;
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);
@@ -1490,7 +1566,7 @@ cudaError_t soft_assemble(pcc_ctx* ctx) {
   if (ctx->n) {
     k_soft_cell<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.view(), (long long)ctx->n, ctx->cons.view(),
                                                     ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p, ctx->params.xi,
-                                                    ctx->params.lambda, ctx->params.tau, 0.0, 0);
+                                                    ctx->params.lambda, ctx->params.tau, 0.0, 0, nullptr);
     ctx->launches++;
   }
   return cudaGetLastError();
@@ -1509,7 +1585,8 @@ cudaError_t soft_forces_and_move(pcc_ctx* ctx, double dt) {
   if (ctx->n) {
     k_soft_cell<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.view(), (long long)ctx->n, ctx->cons.view(),
                                                     ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p, ctx->params.xi,
-                                                    ctx->params.lambda, ctx->params.tau, dt, 1);
+                                                    ctx->params.lambda, ctx->params.tau, dt, 1,
+                                                    ctx->uext_active ? ctx->uext.p : nullptr);
     ctx->launches++;
   }
   return cudaGetLastError();

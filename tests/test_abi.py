@@ -52,7 +52,7 @@ def test_division_draws_of_device_code_match_libstdcxx():
 def test_create_rejects_bad_parameters():
     lib = device.load_library()
     h = C.c_void_p()
-    p = abi.default_params(temperature=1e-28)
+    p = abi.default_params(temperature=-1.0)
     assert lib.pcc_create(C.byref(p), 0, C.byref(h)) == abi.PCC_ERR_INVALID
     p = abi.default_params(mode=7)
     assert lib.pcc_create(C.byref(p), 0, C.byref(h)) == abi.PCC_ERR_INVALID
