@@ -9,7 +9,7 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-SOURCES = ["pcc_api.cu", "pcc_scan_sort.cu", "pcc_detect.cu", "pcc_solver.cu", "pcc_update.cu", "pcc_noalloc.cu",
+SOURCES = ["pcc_api.cu", "pcc_scan_sort.cu", "pcc_detect.cu", "pcc_solver.cu", "pcc_planar.cu", "pcc_update.cu", "pcc_noalloc.cu",
            "pcc_serve.cu", "pcc_vtk.cu"]
 OUT = PKG / "libpcc_gpu.so"
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -1,0 +1,192 @@
+// Device helpers shared by the BBPGD kernels (general 3D form in
+// pcc_solver.cu, planar forms in pcc_planar.cu): the projection, PETSc's
+// VecScale special cases, the bounded grid barriers, the projected-gradient
+// residual term, the Barzilai-Borwein step and the BBPGD trace record.
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+
+#include "pcc_kernels.hpp"
+
+namespace pcc {
+
+constexpr long long kSpinLimit = 1LL << 26;
+constexpr int kTraceWidth = 8;  // it, residual, step size, linear, quadratic, growth, total, -
+
+// gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0): VecWAXPY with PETSc's special
+// cases for the coefficient, then VecPointwiseMax against 0.
+__device__ __forceinline__ double project(double gp, double g, double alpha) {
+  const double a = -alpha;
+  double v;
+  if (a == 1.0) v = add(gp, g);
+  else if (a == -1.0) v = sub(gp, g);
+  else if (a == 0.0) v = gp;
+  else v = add(mul(a, g), gp);
+  return v < 0.0 ? 0.0 : v;
+}
+
+// VecScale(x, a) for one entry.
+__device__ __forceinline__ double vscale(double a, double x) {
+  if (a == 1.0) return x;
+  if (a == 0.0) return 0.0;
+  return mul(a, x);
+}
+
+__device__ __forceinline__ bool barrier(SolverScalars* sc, unsigned nblocks, DevStatus* st) {
+  if (nblocks == 1) {  // one block: a block barrier orders its global writes
+    __syncthreads();
+    return true;
+  }
+  __shared__ unsigned s_gen;
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_ok = 1;
+    s_gen = *(volatile unsigned*)&sc->gen;
+    __threadfence();
+    unsigned t = atomicAdd(&sc->count, 1u);
+    if (t == nblocks - 1) {
+      sc->count = 0;
+      __threadfence();
+      atomicAdd(&sc->gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*(volatile unsigned*)&sc->gen == s_gen) {
+        __nanosleep(40);
+        if (++spins > kSpinLimit) {
+          raise_error(st, kDevErrTimeout, 20);
+          s_ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+// Barrier whose last arriving block first runs `reduce` (all its threads).
+template <typename R>
+__device__ __forceinline__ bool barrier_reduce(SolverScalars* sc, unsigned nblocks, DevStatus* st, R reduce) {
+  if (nblocks == 1) {
+    __syncthreads();
+    reduce();
+    __syncthreads();
+    return true;
+  }
+  __shared__ unsigned s_gen;
+  __shared__ int s_last, s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_ok = 1;
+    s_gen = *(volatile unsigned*)&sc->gen;
+    __threadfence();
+    unsigned t = atomicAdd(&sc->count, 1u);
+    s_last = (t == nblocks - 1);
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    reduce();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sc->count = 0;
+      __threadfence();
+      atomicAdd(&sc->gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    long long spins = 0;
+    while (*(volatile unsigned*)&sc->gen == s_gen) {
+      __nanosleep(40);
+      if (++spins > kSpinLimit) {
+        raise_error(st, kDevErrTimeout, 21);
+        s_ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+__device__ __forceinline__ double proj_grad_abs(double g, double gam) {
+  double v = gam > 0 ? g : (g < 0.0 ? g : 0.0);
+  return fabs(v);
+}
+
+// Fixed-shape block reduction of 4 values (sum, sum, sum, max).
+__device__ __forceinline__ void block_reduce4(double v[4], double* sm) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) sm[q * kBlock + t] = v[q];
+  __syncthreads();
+  for (int w = kBlock / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      sm[t] = add(sm[t], sm[t + w]);
+      sm[kBlock + t] = add(sm[kBlock + t], sm[kBlock + t + w]);
+      sm[2 * kBlock + t] = add(sm[2 * kBlock + t], sm[2 * kBlock + t + w]);
+      double x = sm[3 * kBlock + t], y = sm[3 * kBlock + t + w];
+      sm[3 * kBlock + t] = x < y ? y : x;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = sm[q * kBlock];
+  __syncthreads();
+}
+
+// Energy of the BBPGD trace (HardModelGradient::energy, HardModelGradient.cpp:160-203)
+// from the block partials of the cell terms and the chunk partials of the
+// linear term; written by the last block of a barrier.
+__device__ __forceinline__ void trace_record(double* sm, const double* tr_part, unsigned nb, long long nchunks,
+                                             double dt, double lambda, double tau, long long it, double res,
+                                             double alpha, double* out, long long cap) {
+  double v[4] = {0, 0, 0, 0};
+  for (long long b = threadIdx.x; b < (long long)nb; b += kBlock) {
+    v[0] = add(v[0], ldcg(tr_part + 2 * b));
+    v[1] = add(v[1], ldcg(tr_part + 2 * b + 1));
+  }
+  for (long long ch = threadIdx.x; ch < nchunks; ch += kBlock) v[2] = add(v[2], ldcg(tr_part + 2 * nb + ch));
+  block_reduce4(v, sm);
+  if (threadIdx.x == 0 && it < cap) {
+    const double lin = v[2];
+    const double quad = mul(v[0], dvd(dt, 2.0));
+    const double growth = mul(v[1], dvd(dt, mul(lambda, tau)));
+    double* r = out + (long long)kTraceWidth * it;
+    r[0] = (double)it;
+    r[1] = res;
+    r[2] = alpha;
+    r[3] = lin;
+    r[4] = quad;
+    r[5] = growth;
+    r[6] = add(add(lin, quad), growth);
+    r[7] = 0.0;
+  }
+}
+
+// Step size of the next iteration from the reduced sums (sum dgam^2,
+// sum dgam*dg, sum dg^2): BB1 on even, BB2 on odd iterations
+// (solver/BBPGD.cpp:98-112), with the reference's +10 eps guard on a tiny
+// denominator.  Both BB quotients are >= 0 in exact arithmetic (the gradient
+// is monotone); near convergence rounding can make the numerator a tiny
+// negative number, and a negative step lifts an inactive constraint to
+// gamma ~ 1e-26 > 0, where the projected residual counts its full positive
+// gradient and never returns below tol.  The step is clamped at 0.
+__device__ __forceinline__ double bb_step(const double v[4], long long it) {
+  double num, den;
+  if (it % 2 == 0) {
+    num = v[0];
+    den = v[1];
+  } else {
+    den = v[2];
+    num = v[1];
+  }
+  if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
+  const double step = dvd(num, den);
+  return step > 0.0 ? step : 0.0;
+}
+
+}  // namespace pcc

@@ -119,9 +119,10 @@ struct pcc_ctx {
   pcc::DevBuf<pcc::SolverScalars> scal;
   pcc::DevBuf<double> fel;  // soft: Hertz force magnitude per contact
   // packed operands of the planar solver
-  pcc::DevBuf<int2> p_ij;
-  pcc::DevBuf<double2> p_n, p_t, p_s;
-  pcc::DevBuf<double4> p_st0, p_st1, p_inc, p_cell, p_u;
+  pcc::DevBuf<int2> p_ij, p_pos;
+  pcc::DevBuf<double2> p_n, p_t, p_s, p_gg0, p_gg1, p_ev0, p_ev1;
+  pcc::DevBuf<double> p_gold;
+  pcc::DevBuf<double4> p_inc, p_cell, p_u;
   // ... their FP32 forms (mixed precision)
   pcc::DevBuf<float2> pf_n, pf_t, pf_s;
   pcc::DevBuf<float4> pf_inc, pf_cell, pf_u;
@@ -156,6 +157,8 @@ struct pcc_ctx {
   int coop_blocks = 0;         // co-resident blocks of the general solver kernel
   int coop_blocks_planar = 0;  // ... of the planar one
   int coop_blocks_mixed = 0;   // ... of its mixed-precision form
+  int coop_planar_tr = 0;      // ... and of their traced forms
+  int coop_mixed_tr = 0;
 
   // VTK output: device snapshot, side stream and background writer
   pcc::DevBuf<double> vtk_dev;

@@ -40,6 +40,21 @@ cudaError_t soft_forces_and_move(pcc_ctx* ctx, double dt);
 // Soft model force assembly only (frozen microbench).
 cudaError_t soft_assemble(pcc_ctx* ctx);
 
+// ---- pcc_planar.cu
+// BBPGD trace buffers handed to the planar solver (trace = 0: none).
+struct PlanarTrace {
+  int trace;
+  double* tr_part;
+  double* trace_out;
+  long long trace_cap;
+};
+// Constraint chunks of the planar solver's reductions for m constraints.
+long long planar_chunks(size_t m);
+// Packs the planar operands and launches the planar BBPGD solve on the
+// context's stream (FP64, or mixed precision); *kind = 1 for the multi-block
+// cooperative kernel, 0 for a one-block launch.
+cudaError_t planar_bbpgd(pcc_ctx* ctx, double dt, bool mixed, const PlanarTrace& tr, int* kind);
+
 // ---- pcc_update.cu
 cudaError_t reset_ldot(pcc_ctx* ctx);
 cudaError_t grow_cells(pcc_ctx* ctx, double dt);

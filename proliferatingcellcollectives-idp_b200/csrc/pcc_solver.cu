@@ -18,6 +18,7 @@
 #include <cfloat>
 #include <cmath>
 
+#include "pcc_bbpgd.cuh"
 #include "pcc_kernels.hpp"
 
 namespace pcc {
@@ -26,12 +27,9 @@ namespace {
 
 constexpr int kChunk = 1024;            // constraints per reduction chunk
 constexpr int kPerThread = kChunk / kBlock;
-constexpr long long kSpinLimit = 1LL << 26;
 // A measured colony of 1,309 cells iterated faster over several SMs than in
 // one 1024-thread CTA, so the one-CTA form stops where one block would
 // otherwise hold the whole colony anyway.
-constexpr int kSmallCells = 1024;         // planar: one 1024-thread CTA up to this many cells ...
-constexpr int kSmallConstraints = 4096;   // ... and constraints
 constexpr int kOneBlockCells = 1024;      // otherwise one 256-thread block up to this many cells ...
 constexpr int kOneBlockConstraints = 4096;  // ... and constraints
 
@@ -64,106 +62,7 @@ struct SolverArgs {
   long long trace_cap; // iterations that fit
 };
 
-constexpr int kTraceWidth = 8;  // it, residual, step size, linear, quadratic, growth, total, -
 
-
-// gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0): VecWAXPY with PETSc's special
-// cases for the coefficient, then VecPointwiseMax against 0.
-__device__ __forceinline__ double project(double gp, double g, double alpha) {
-  const double a = -alpha;
-  double v;
-  if (a == 1.0) v = add(gp, g);
-  else if (a == -1.0) v = sub(gp, g);
-  else if (a == 0.0) v = gp;
-  else v = add(mul(a, g), gp);
-  return v < 0.0 ? 0.0 : v;
-}
-
-// VecScale(x, a) for one entry.
-__device__ __forceinline__ double vscale(double a, double x) {
-  if (a == 1.0) return x;
-  if (a == 0.0) return 0.0;
-  return mul(a, x);
-}
-
-__device__ __forceinline__ bool barrier(SolverScalars* sc, unsigned nblocks, DevStatus* st) {
-  if (nblocks == 1) {  // one block: a block barrier orders its global writes
-    __syncthreads();
-    return true;
-  }
-  __shared__ unsigned s_gen;
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_ok = 1;
-    s_gen = *(volatile unsigned*)&sc->gen;
-    __threadfence();
-    unsigned t = atomicAdd(&sc->count, 1u);
-    if (t == nblocks - 1) {
-      sc->count = 0;
-      __threadfence();
-      atomicAdd(&sc->gen, 1u);
-    } else {
-      long long spins = 0;
-      while (*(volatile unsigned*)&sc->gen == s_gen) {
-        __nanosleep(40);
-        if (++spins > kSpinLimit) {
-          raise_error(st, kDevErrTimeout, 20);
-          s_ok = 0;
-          break;
-        }
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return s_ok;
-}
-
-// Barrier whose last arriving block first runs `reduce` (all its threads).
-template <typename R>
-__device__ __forceinline__ bool barrier_reduce(SolverScalars* sc, unsigned nblocks, DevStatus* st, R reduce) {
-  if (nblocks == 1) {
-    __syncthreads();
-    reduce();
-    __syncthreads();
-    return true;
-  }
-  __shared__ unsigned s_gen;
-  __shared__ int s_last, s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_ok = 1;
-    s_gen = *(volatile unsigned*)&sc->gen;
-    __threadfence();
-    unsigned t = atomicAdd(&sc->count, 1u);
-    s_last = (t == nblocks - 1);
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    reduce();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      sc->count = 0;
-      __threadfence();
-      atomicAdd(&sc->gen, 1u);
-    }
-  } else if (threadIdx.x == 0) {
-    long long spins = 0;
-    while (*(volatile unsigned*)&sc->gen == s_gen) {
-      __nanosleep(40);
-      if (++spins > kSpinLimit) {
-        raise_error(st, kDevErrTimeout, 21);
-        s_ok = 0;
-        break;
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return s_ok;
-}
 
 // Pass A for cell p.  mode 0: gamma = gamma_0; mode 1: gamma_k projected from
 // (gam_prev, g_prev, alpha).  Writes U and dldot; with `final` also F, sigma,
@@ -261,61 +160,6 @@ __device__ __forceinline__ double constraint_grad(const SolverArgs& a, long long
   }
   // VecMAXPY(phi_next, {dt, -dt}, {phidot, growth})
   return add(a.phi[c], add(mul(a.dt, pd), mul(-a.dt, gr)));
-}
-
-__device__ __forceinline__ double proj_grad_abs(double g, double gam) {
-  double v = gam > 0 ? g : (g < 0.0 ? g : 0.0);
-  return fabs(v);
-}
-
-// Fixed-shape block reduction of 4 values (sum, sum, sum, max).
-__device__ __forceinline__ void block_reduce4(double v[4], double* sm) {
-  const int t = threadIdx.x;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) sm[q * kBlock + t] = v[q];
-  __syncthreads();
-  for (int w = kBlock / 2; w > 0; w >>= 1) {
-    if (t < w) {
-      sm[t] = add(sm[t], sm[t + w]);
-      sm[kBlock + t] = add(sm[kBlock + t], sm[kBlock + t + w]);
-      sm[2 * kBlock + t] = add(sm[2 * kBlock + t], sm[2 * kBlock + t + w]);
-      double x = sm[3 * kBlock + t], y = sm[3 * kBlock + t + w];
-      sm[3 * kBlock + t] = x < y ? y : x;
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) v[q] = sm[q * kBlock];
-  __syncthreads();
-}
-
-// Energy of the BBPGD trace (HardModelGradient::energy, HardModelGradient.cpp:160-203)
-// from the block partials of the cell terms and the chunk partials of the
-// linear term; written by the last block of a barrier.
-__device__ __forceinline__ void trace_record(double* sm, const double* tr_part, unsigned nb, long long nchunks,
-                                             double dt, double lambda, double tau, long long it, double res,
-                                             double alpha, double* out, long long cap) {
-  double v[4] = {0, 0, 0, 0};
-  for (long long b = threadIdx.x; b < (long long)nb; b += kBlock) {
-    v[0] = add(v[0], ldcg(tr_part + 2 * b));
-    v[1] = add(v[1], ldcg(tr_part + 2 * b + 1));
-  }
-  for (long long ch = threadIdx.x; ch < nchunks; ch += kBlock) v[2] = add(v[2], ldcg(tr_part + 2 * nb + ch));
-  block_reduce4(v, sm);
-  if (threadIdx.x == 0 && it < cap) {
-    const double lin = v[2];
-    const double quad = mul(v[0], dvd(dt, 2.0));
-    const double growth = mul(v[1], dvd(dt, mul(lambda, tau)));
-    double* r = out + (long long)kTraceWidth * it;
-    r[0] = (double)it;
-    r[1] = res;
-    r[2] = alpha;
-    r[3] = lin;
-    r[4] = quad;
-    r[5] = growth;
-    r[6] = add(add(lin, quad), growth);
-    r[7] = 0.0;
-  }
 }
 
 // Block partials of the cell energy terms (all threads of the block call).
@@ -456,25 +300,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
           // a recording-only trace (trace == 2) keeps the every-10th test
           if (v[3] <= a.tol && (TR != 2 || it % 10 == 0)) conv = 1;
         }
-        if (!conv) {
-          // BB1 on even, BB2 on odd iterations (BBPGD.cpp:98-112)
-          double num, den;
-          if (it % 2 == 0) {
-            num = v[0];
-            den = v[1];
-          } else {
-            den = v[2];
-            num = v[1];
-          }
-          if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
-          // Both BB quotients are >= 0 in exact arithmetic (the gradient is
-          // monotone); near convergence rounding can make the numerator a tiny
-          // negative number, and a negative step lifts an inactive constraint
-          // to gamma ~ 1e-26 > 0, where the projected residual counts its full
-          // positive gradient and never returns below tol.  Clamp at 0.
-          const double step = dvd(num, den);
-          sc->alpha = step > 0.0 ? step : 0.0;
-        }
+        if (!conv) sc->alpha = bb_step(v, it);  // BBPGD.cpp:98-112
         sc->converged = conv;
         sc->iterations = it;
       }
@@ -491,546 +317,6 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
     a.gamma[c] = ldcg(a.gam[p] + c);
     a.phi[c] = ldcg(a.g[1 - p] + c);
   }
-}
-
-// ---------------------------------------------------------------- planar form
-// For a planar colony the D row of a constraint has three non-zero entries per
-// side (n_x, n_y and the z torque arm) and U three per cell (u_x, u_y, w_z);
-// every other term of the general kernel is an exact zero, and a running sum
-// that starts at +0 is unchanged by adding a signed zero, so skipping them
-// gives bit-identical results.  Operands are packed so each gather is one
-// sector:
-//   per incidence entry  inc  = (D_x, D_y, D_t, s) of that side,
-//   per constraint       st   = (gamma, g, gamma_old, 0), ping-pong per iteration,
-//                        ij, n = (n_x, n_y), t = (t_iz, t_jz), s = (s_i, s_j),
-//   per cell             cell = (M_lin, M_rot, len, ldot_prev), u = (u_x, u_y, w_z, dldot).
-// Real = double is the plain FP64 method.  Real = float is the mixed-precision
-// form: the D, L and M entries, U and the D / M products are FP32 (half the
-// operand bytes), while gamma, the gradient, Phi / phi_next, the stress sum
-// sigma = L^T gamma, the BB dot products and the residual stay FP64.
-template <class Real>
-struct PlanarTypes;
-template <>
-struct PlanarTypes<double> {
-  using V2 = double2;
-  using V4 = double4;
-};
-template <>
-struct PlanarTypes<float> {
-  using V2 = float2;
-  using V4 = float4;
-};
-
-__device__ __forceinline__ double4 mk4(double a, double b, double c, double d, double*) {
-  return make_double4(a, b, c, d);
-}
-__device__ __forceinline__ float4 mk4(double a, double b, double c, double d, float*) {
-  return make_float4((float)a, (float)b, (float)c, (float)d);
-}
-
-template <class Real>
-struct PlanarArgs {
-  using V2 = typename PlanarTypes<Real>::V2;
-  using V4 = typename PlanarTypes<Real>::V4;
-  long long m, n;
-  const int2* ij;
-  const V2 *nn, *tt, *ss;
-  double* phi;    // Phi on entry, phi_next on exit
-  double* gamma;  // gamma_0 on entry, gamma_{k-1} on exit
-  double4* st[2];
-  const int *inc_off, *inc_ent;
-  const V4 *inc, *cell;
-  const double* uext;  // rotational U_ext, 3 per cell (only z is used: monolayer kicks); null: zero
-  V4* u;
-  double *U, *F, *sig, *ldot, *imp;  // general-layout outputs on residual iterations
-  double dt, lambda, tau, tol;
-  long long max_it;
-  double* partials;
-  long long nchunks;
-  SolverScalars* sc;
-  DevStatus* st_err;
-  int trace;  // BBPGD trace, as in SolverArgs
-  double* tr_part;
-  double* trace_out;
-  long long trace_cap;
-};
-
-template <class Real>
-__device__ __forceinline__ void planar_cell_pass(const PlanarArgs<Real>& a, long long p, int mode,
-                                                 const double4* stp, double alpha, bool final, double* eq = nullptr,
-                                                 double* eg = nullptr) {
-  constexpr bool kF64 = sizeof(Real) == 8;
-  Real f0 = 0, f1 = 0, f5 = 0;
-  double g0 = 0, g1 = 0, g5 = 0;  // D^T gamma (trace only)
-  double sg = 0.0;
-  const int b = a.inc_off[p], e = a.inc_off[p + 1];
-#pragma unroll 4
-  for (int k = b; k < e; ++k) {
-    const long long c = a.inc_ent[k] >> 1;
-    const auto d = a.inc[k];
-    const double4 s = ldcg(stp + c);
-    const double gc = mode == 0 ? s.z : project(s.x, s.y, alpha);
-    const double diff = sub(gc, s.z);
-    if constexpr (kF64) {
-      f0 = add(f0, mul(d.x, diff));
-      f1 = add(f1, mul(d.y, diff));
-      f5 = add(f5, mul(d.z, diff));
-      sg = add(sg, mul(d.w, gc));
-    } else {
-      const float df = (float)diff;
-      f0 = fmaf(d.x, df, f0);
-      f1 = fmaf(d.y, df, f1);
-      f5 = fmaf(d.z, df, f5);
-      sg = fma((double)d.w, gc, sg);
-    }
-    if (eq) {
-      g0 = add(g0, mul((double)d.x, gc));
-      g1 = add(g1, mul((double)d.y, gc));
-      g5 = add(g5, mul((double)d.z, gc));
-    }
-  }
-  const auto cl = a.cell[p];
-  double ux, uy, wz;
-  const double ldp = cl.w;
-  const double uez = a.uext ? a.uext[3 * p + 2] : 0.0;
-  if constexpr (kF64) {
-    ux = add(add(0.0, mul(cl.x, f0)), 0.0);
-    uy = add(add(0.0, mul(cl.x, f1)), 0.0);
-    wz = add(add(0.0, mul(cl.y, f5)), uez);
-  } else {
-    ux = cl.x * f0;
-    uy = cl.x * f1;
-    wz = (double)(cl.y * f5) + uez;
-  }
-  const double im = exp(vscale(-a.lambda, sg));
-  const double ld = vscale(dvd(1.0, a.tau), mul((double)cl.z, im));
-  a.u[p] = mk4(ux, uy, wz, sub(ld, ldp), (Real*)nullptr);
-  if (eq) {
-    const double ml = cl.x, mr = cl.y;
-    *eq = add(*eq, add(add(mul(g0, mul(ml, g0)), mul(g1, mul(ml, g1))), mul(g5, mul(mr, g5))));
-    *eg = add(*eg, mul((double)cl.z, im));
-  }
-  if (final) {
-    double* U = a.U + 6 * p;
-    double* F = a.F + 6 * p;
-    U[0] = ux;
-    U[1] = uy;
-    U[2] = 0.0;
-    U[3] = 0.0;
-    U[4] = 0.0;
-    U[5] = wz;
-    F[0] = f0;
-    F[1] = f1;
-    F[2] = 0.0;
-    F[3] = 0.0;
-    F[4] = 0.0;
-    F[5] = f5;
-    a.sig[p] = sg;
-    a.ldot[p] = ld;
-    a.imp[p] = im;
-  }
-}
-
-template <class Real>
-__device__ __forceinline__ double planar_grad(const PlanarArgs<Real>& a, long long c) {
-  const int2 ij = a.ij[c];
-  const auto n = a.nn[c];
-  const auto t = a.tt[c];
-  const auto s = a.ss[c];
-  const auto ui = ldcg(a.u + ij.x);
-  const auto uj = ldcg(a.u + ij.y);
-  if constexpr (sizeof(Real) == 8) {
-    double pd = 0.0;  // gi < gj: the i block comes first in column order
-    pd = add(pd, mul(n.x, ui.x));
-    pd = add(pd, mul(n.y, ui.y));
-    pd = add(pd, mul(t.x, ui.z));
-    pd = add(pd, mul(-n.x, uj.x));
-    pd = add(pd, mul(-n.y, uj.y));
-    pd = add(pd, mul(t.y, uj.z));
-    double gr = 0.0;
-    gr = add(gr, mul(s.x, ui.w));
-    gr = add(gr, mul(s.y, uj.w));
-    return add(a.phi[c], add(mul(a.dt, pd), mul(-a.dt, gr)));
-  } else {
-    float pd = n.x * ui.x;
-    pd = fmaf(n.y, ui.y, pd);
-    pd = fmaf(t.x, ui.z, pd);
-    pd = fmaf(-n.x, uj.x, pd);
-    pd = fmaf(-n.y, uj.y, pd);
-    pd = fmaf(t.y, uj.z, pd);
-    const float gr = fmaf(s.y, uj.w, s.x * ui.w);
-    return a.phi[c] + a.dt * ((double)pd - (double)gr);
-  }
-}
-
-template <class Real, int kTr>
-__global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PlanarArgs<Real> a) {
-  const int TR = kTr ? a.trace : 0;
-  __shared__ double sm[4 * kBlock];
-  const unsigned nb = gridDim.x;
-  const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
-  const long long stride = (long long)nb * kBlock;
-  SolverScalars* sc = a.sc;
-
-  {
-    double eq = 0.0, eg = 0.0;
-    for (long long p = tid; p < a.n; p += stride)
-      planar_cell_pass(a, p, 0, a.st[0], 0.0, false, TR ? &eq : nullptr, &eg);
-    if (TR) trace_cells(sm, eq, eg, a.tr_part);
-  }
-  if (!barrier(sc, nb, a.st_err)) return;
-  for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
-    double v[4] = {0, 0, 0, 0};
-    double lin = 0.0;
-#pragma unroll
-    for (int k = 0; k < kPerThread; ++k) {
-      const long long c = ch * kChunk + k * kBlock + threadIdx.x;
-      if (c < a.m) {
-        const double g = planar_grad(a, c);
-        const double gm = a.st[0][c].x;
-        a.st[0][c].y = g;
-        double r = proj_grad_abs(g, gm);
-        v[3] = v[3] < r ? r : v[3];
-        if (TR) lin = add(lin, mul(gm, a.phi[c]));
-      }
-    }
-    block_reduce4(v, sm);
-    if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
-    if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
-  }
-  auto reduce_init = [&]() {
-    double v[4] = {0, 0, 0, 0};
-    for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
-      double r = ldcg(a.partials + 4 * ch + 3);
-      v[3] = v[3] < r ? r : v[3];
-    }
-    block_reduce4(v, sm);
-    if (threadIdx.x == 0) {
-      sc->res0 = v[3];
-      sc->residual = v[3];
-      sc->alpha = 1.0 / v[3];
-      sc->converged = 0;
-    }
-    if (TR)
-      trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
-                   a.trace_cap);
-  };
-  if (!barrier_reduce(sc, nb, a.st_err, reduce_init)) return;
-
-  int p = 0;
-  long long it = 1;
-  while (it < a.max_it) {
-    const double alpha = *(volatile double*)&sc->alpha;
-    const bool check = (it % 10) == 0 || TR;
-    const double4* sp = a.st[p];
-    double4* so = a.st[1 - p];
-    {
-      double eq = 0.0, eg = 0.0;
-      for (long long q = tid; q < a.n; q += stride)
-        planar_cell_pass(a, q, 1, sp, alpha, check, TR ? &eq : nullptr, &eg);
-      if (TR) trace_cells(sm, eq, eg, a.tr_part);
-    }
-    if (!barrier(sc, nb, a.st_err)) return;
-    for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
-      double v[4] = {0, 0, 0, 0};
-      double lin = 0.0;
-#pragma unroll
-      for (int k = 0; k < kPerThread; ++k) {
-        const long long c = ch * kChunk + k * kBlock + threadIdx.x;
-        if (c < a.m) {
-          const double4 s = ldcg(sp + c);
-          const double gam = project(s.x, s.y, alpha);
-          const double g = planar_grad(a, c);
-          so[c] = make_double4(gam, g, s.z, 0.0);
-          const double dgm = sub(gam, s.x), dg = sub(g, s.y);
-          v[0] = add(v[0], mul(dgm, dgm));
-          v[1] = add(v[1], mul(dgm, dg));
-          v[2] = add(v[2], mul(dg, dg));
-          if (check) {
-            double r = proj_grad_abs(g, gam);
-            v[3] = v[3] < r ? r : v[3];
-          }
-          if (TR) lin = add(lin, mul(gam, a.phi[c]));
-        }
-      }
-      block_reduce4(v, sm);
-      if (threadIdx.x == 0) {
-        a.partials[4 * ch + 0] = v[0];
-        a.partials[4 * ch + 1] = v[1];
-        a.partials[4 * ch + 2] = v[2];
-        a.partials[4 * ch + 3] = v[3];
-      }
-      if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
-    }
-    auto reduce_iter = [&]() {
-      double v[4] = {0, 0, 0, 0};
-      for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
-        v[0] = add(v[0], ldcg(a.partials + 4 * ch + 0));
-        v[1] = add(v[1], ldcg(a.partials + 4 * ch + 1));
-        v[2] = add(v[2], ldcg(a.partials + 4 * ch + 2));
-        double r = ldcg(a.partials + 4 * ch + 3);
-        v[3] = v[3] < r ? r : v[3];
-      }
-      block_reduce4(v, sm);
-      if (TR)
-        trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, it, v[3], alpha, a.trace_out,
-                     a.trace_cap);
-      if (threadIdx.x == 0) {
-        int conv = 0;
-        if (check) {
-          sc->residual = v[3];
-          // a recording-only trace (trace == 2) keeps the every-10th test
-          if (v[3] <= a.tol && (TR != 2 || it % 10 == 0)) conv = 1;
-        }
-        if (!conv) {
-          double num, den;
-          if (it % 2 == 0) {
-            num = v[0];
-            den = v[1];
-          } else {
-            den = v[2];
-            num = v[1];
-          }
-          if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
-          // Both BB quotients are >= 0 in exact arithmetic (the gradient is
-          // monotone); near convergence rounding can make the numerator a tiny
-          // negative number, and a negative step lifts an inactive constraint
-          // to gamma ~ 1e-26 > 0, where the projected residual counts its full
-          // positive gradient and never returns below tol.  Clamp at 0.
-          const double step = dvd(num, den);
-          sc->alpha = step > 0.0 ? step : 0.0;
-        }
-        sc->converged = conv;
-        sc->iterations = it;
-      }
-    };
-    if (!barrier_reduce(sc, nb, a.st_err, reduce_iter)) return;
-    if (*(volatile int*)&sc->converged) break;
-    p = 1 - p;
-    ++it;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) sc->iterations = it;
-  if (!*(volatile int*)&sc->converged) return;
-  for (long long c = tid; c < a.m; c += stride) {
-    a.gamma[c] = ldcg(a.st[p] + c).x;
-    a.phi[c] = ldcg(a.st[1 - p] + c).y;
-  }
-}
-
-// ------------------------------------------------------- one-CTA form, small colonies
-// A planar colony of up to kSmallCells cells and kSmallConstraints constraints runs
-// its whole BBPGD in one 1024-thread block: four 256-thread groups share the
-// work, each group reduces the chunks it owns with its own named barrier and
-// the same tree as block_reduce4, and group 0 reduces the chunk partials in
-// the same order as the multi-block kernel.  Every value is therefore the
-// multi-block kernel's, bit for bit; the iteration costs block barriers
-// instead of grid barriers and four times the threads of the one-block launch.
-constexpr int kSmallThreads = 4 * kBlock;
-constexpr int kSmallGroups = kSmallThreads / kBlock;
-
-__device__ __forceinline__ void group_sync(int grp) {
-  asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(kBlock) : "memory");
-}
-
-__device__ __forceinline__ void group_reduce4(double v[4], double* sm, int grp) {
-  const int t = threadIdx.x & (kBlock - 1);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) sm[q * kBlock + t] = v[q];
-  group_sync(grp);
-  for (int w = kBlock / 2; w > 0; w >>= 1) {
-    if (t < w) {
-      sm[t] = add(sm[t], sm[t + w]);
-      sm[kBlock + t] = add(sm[kBlock + t], sm[kBlock + t + w]);
-      sm[2 * kBlock + t] = add(sm[2 * kBlock + t], sm[2 * kBlock + t + w]);
-      double x = sm[3 * kBlock + t], y = sm[3 * kBlock + t + w];
-      sm[3 * kBlock + t] = x < y ? y : x;
-    }
-    group_sync(grp);
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) v[q] = sm[q * kBlock];
-  group_sync(grp);
-}
-
-template <class Real>
-__global__ void __launch_bounds__(kSmallThreads, 1) k_bbpgd_planar_small(PlanarArgs<Real> a) {
-  __shared__ double sm[kSmallGroups][4 * kBlock];
-  __shared__ double s_alpha;
-  __shared__ int s_conv;
-  const int grp = threadIdx.x / kBlock, lane = threadIdx.x % kBlock;
-  SolverScalars* sc = a.sc;
-
-  for (long long p = threadIdx.x; p < a.n; p += kSmallThreads) planar_cell_pass(a, p, 0, a.st[0], 0.0, false);
-  __syncthreads();
-  for (long long ch = grp; ch < a.nchunks; ch += kSmallGroups) {
-    double v[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < kPerThread; ++k) {
-      const long long c = ch * kChunk + k * kBlock + lane;
-      if (c < a.m) {
-        const double g = planar_grad(a, c);
-        const double gm = a.st[0][c].x;
-        a.st[0][c].y = g;
-        double r = proj_grad_abs(g, gm);
-        v[3] = v[3] < r ? r : v[3];
-      }
-    }
-    group_reduce4(v, sm[grp], grp);
-    if (lane == 0) a.partials[4 * ch + 3] = v[3];
-  }
-  __syncthreads();
-  if (grp == 0) {
-    double v[4] = {0, 0, 0, 0};
-    for (long long ch = lane; ch < a.nchunks; ch += kBlock) {
-      double r = ldcg(a.partials + 4 * ch + 3);
-      v[3] = v[3] < r ? r : v[3];
-    }
-    group_reduce4(v, sm[0], 0);
-    if (lane == 0) {
-      sc->res0 = v[3];
-      sc->residual = v[3];
-      s_alpha = 1.0 / v[3];
-      s_conv = 0;
-    }
-  }
-  __syncthreads();
-
-  int p = 0;
-  long long it = 1;
-  while (it < a.max_it) {
-    const double alpha = s_alpha;
-    const bool check = (it % 10) == 0;
-    const double4* sp = a.st[p];
-    double4* so = a.st[1 - p];
-    for (long long q = threadIdx.x; q < a.n; q += kSmallThreads) planar_cell_pass(a, q, 1, sp, alpha, check);
-    __syncthreads();
-    for (long long ch = grp; ch < a.nchunks; ch += kSmallGroups) {
-      double v[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (int k = 0; k < kPerThread; ++k) {
-        const long long c = ch * kChunk + k * kBlock + lane;
-        if (c < a.m) {
-          const double4 s = ldcg(sp + c);
-          const double gam = project(s.x, s.y, alpha);
-          const double g = planar_grad(a, c);
-          so[c] = make_double4(gam, g, s.z, 0.0);
-          const double dgm = sub(gam, s.x), dg = sub(g, s.y);
-          v[0] = add(v[0], mul(dgm, dgm));
-          v[1] = add(v[1], mul(dgm, dg));
-          v[2] = add(v[2], mul(dg, dg));
-          if (check) {
-            double r = proj_grad_abs(g, gam);
-            v[3] = v[3] < r ? r : v[3];
-          }
-        }
-      }
-      group_reduce4(v, sm[grp], grp);
-      if (lane == 0) {
-        a.partials[4 * ch + 0] = v[0];
-        a.partials[4 * ch + 1] = v[1];
-        a.partials[4 * ch + 2] = v[2];
-        a.partials[4 * ch + 3] = v[3];
-      }
-    }
-    __syncthreads();
-    if (grp == 0) {
-      double v[4] = {0, 0, 0, 0};
-      for (long long ch = lane; ch < a.nchunks; ch += kBlock) {
-        v[0] = add(v[0], ldcg(a.partials + 4 * ch + 0));
-        v[1] = add(v[1], ldcg(a.partials + 4 * ch + 1));
-        v[2] = add(v[2], ldcg(a.partials + 4 * ch + 2));
-        double r = ldcg(a.partials + 4 * ch + 3);
-        v[3] = v[3] < r ? r : v[3];
-      }
-      group_reduce4(v, sm[0], 0);
-      if (lane == 0) {
-        int conv = 0;
-        if (check) {
-          sc->residual = v[3];
-          if (v[3] <= a.tol) conv = 1;
-        }
-        if (!conv) {
-          double num, den;
-          if (it % 2 == 0) {
-            num = v[0];
-            den = v[1];
-          } else {
-            den = v[2];
-            num = v[1];
-          }
-          if (fabs(den) < 10 * DBL_EPSILON) den = add(den, 10 * DBL_EPSILON);
-          const double step = dvd(num, den);  // clamped at 0 as in k_bbpgd_planar
-          s_alpha = step > 0.0 ? step : 0.0;
-        }
-        s_conv = conv;
-        sc->iterations = it;
-      }
-    }
-    __syncthreads();
-    if (s_conv) break;
-    p = 1 - p;
-    ++it;
-  }
-  if (threadIdx.x == 0) {
-    sc->iterations = it;
-    sc->converged = s_conv;
-    sc->alpha = s_alpha;
-  }
-  if (!s_conv) return;
-  for (long long c = threadIdx.x; c < a.m; c += kSmallThreads) {
-    a.gamma[c] = ldcg(a.st[p] + c).x;
-    a.phi[c] = ldcg(a.st[1 - p] + c).y;
-  }
-}
-
-// Packs the planar operands of one ReLCP phase.
-template <class V2>
-__device__ __forceinline__ V2 mk2(double a, double b);
-template <>
-__device__ __forceinline__ double2 mk2<double2>(double a, double b) {
-  return make_double2(a, b);
-}
-template <>
-__device__ __forceinline__ float2 mk2<float2>(double a, double b) {
-  return make_float2((float)a, (float)b);
-}
-
-template <class Real>
-__global__ void k_pack_planar_cons(ConsView cs, long long m, int2* __restrict__ ij,
-                                   typename PlanarTypes<Real>::V2* __restrict__ nn,
-                                   typename PlanarTypes<Real>::V2* __restrict__ tt,
-                                   typename PlanarTypes<Real>::V2* __restrict__ ss, double4* __restrict__ st) {
-  using V2 = typename PlanarTypes<Real>::V2;
-  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m) return;
-  ij[c] = make_int2(cs.gi[c], cs.gj[c]);
-  nn[c] = mk2<V2>(cs.nx[c], cs.ny[c]);
-  tt[c] = mk2<V2>(cs.tiz[c], cs.tjz[c]);
-  ss[c] = mk2<V2>(cs.si[c], cs.sj[c]);
-  const double g = cs.gamma[c];
-  st[c] = make_double4(g, 0.0, g, 0.0);
-}
-
-template <class Real>
-__global__ void k_pack_planar_inc(ConsView cs, const int* __restrict__ inc_ent, long long ne,
-                                  typename PlanarTypes<Real>::V4* __restrict__ inc) {
-  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ne) return;
-  const int ent = inc_ent[k];
-  const long long c = ent >> 1;
-  if ((ent & 1) == 0)
-    inc[k] = mk4(cs.nx[c], cs.ny[c], cs.tiz[c], cs.si[c], (Real*)nullptr);
-  else
-    inc[k] = mk4(-cs.nx[c], -cs.ny[c], cs.tjz[c], cs.sj[c], (Real*)nullptr);
-}
-
-template <class Real>
-__global__ void k_pack_planar_cells(const double* __restrict__ Ml, const double* __restrict__ Mr,
-                                    const double* __restrict__ len, const double* __restrict__ ldot_prev, long long n,
-                                    typename PlanarTypes<Real>::V4* __restrict__ cell) {
-  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  cell[p] = mk4(Ml[p], Mr[p], len[p], ldot_prev[p], (Real*)nullptr);
 }
 
 // Cell update after a solve: dC = G U (Physics.cpp:220-265), Euler step and
@@ -1282,206 +568,116 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   const size_t n = ctx->n, m = ctx->ncons;
   cudaError_t e;
   const size_t mm = m + 1, nn = n + 1;
-  if ((e = ctx->gam_a.reserve(mm, 0, s)) || (e = ctx->gam_b.reserve(mm, 0, s)) || (e = ctx->g_a.reserve(mm, 0, s)) ||
-      (e = ctx->g_b.reserve(mm, 0, s)))
-    return e;
   if ((e = ctx->U.reserve(6 * nn, 0, s)) || (e = ctx->dldot.reserve(nn, 0, s)) || (e = ctx->F.reserve(6 * nn, 0, s)) ||
       (e = ctx->sig.reserve(nn, 0, s)) || (e = ctx->ldot_new.reserve(nn, 0, s)) || (e = ctx->imp_new.reserve(nn, 0, s)))
     return e;
-  const long long nchunks = (long long)((m + kChunk - 1) / kChunk);
-  if ((e = ctx->partials.reserve(4 * (nchunks + 1), 0, s))) return e;
   if ((e = ctx->scal.reserve(1, 0, s))) return e;
   cudaMemsetAsync(ctx->scal.p, 0, sizeof(SolverScalars), s);
-
-  SolverArgs a;
-  ConsView cv = ctx->cons.view();
-  a.m = (long long)m;
-  a.gi = cv.gi;
-  a.gj = cv.gj;
-  a.nx = cv.nx;
-  a.ny = cv.ny;
-  a.nz = cv.nz;
-  a.tix = cv.tix;
-  a.tiy = cv.tiy;
-  a.tiz = cv.tiz;
-  a.tjx = cv.tjx;
-  a.tjy = cv.tjy;
-  a.tjz = cv.tjz;
-  a.si = cv.si;
-  a.sj = cv.sj;
-  a.phi = cv.sd;
-  a.gamma = cv.gamma;
-  a.gam[0] = ctx->gam_a.p;
-  a.gam[1] = ctx->gam_b.p;
-  a.g[0] = ctx->g_a.p;
-  a.g[1] = ctx->g_b.p;
-  a.n = (long long)n;
-  a.inc_off = ctx->inc_off.p;
-  a.inc_ent = ctx->inc_ent.p;
-  a.Mlin = ctx->Mlin.p;
-  a.Mrot = ctx->Mrot.p;
-  a.len = ctx->cells.len.p;
-  a.ldot_prev = ctx->cells.ldot.p;
-  a.uext = ctx->uext_active ? ctx->uext.p : nullptr;
-  a.U = ctx->U.p;
-  a.dl = ctx->dldot.p;
-  a.F = ctx->F.p;
-  a.sig = ctx->sig.p;
-  a.ldot = ctx->ldot_new.p;
-  a.imp = ctx->imp_new.p;
-  a.dt = dt;
-  a.lambda = ctx->params.lambda;
-  a.tau = ctx->params.tau;
-  a.tol = ctx->params.tolerance;
-  a.max_it = ctx->params.max_bbpgd_iterations;
-  a.partials = ctx->partials.p;
-  a.nchunks = nchunks;
-  a.sc = ctx->scal.p;
-  a.st = ctx->status;
+  const long long nchunks = (long long)((m + kChunk - 1) / kChunk);
   const bool tracing = ctx->trace_active;
   long long trace_cap = 0;
   if (tracing) {
     trace_cap = ctx->params.max_bbpgd_iterations + 1;
     if (trace_cap > (1LL << 22)) trace_cap = 1LL << 22;
     if ((e = ctx->trace_dev.reserve((size_t)(kTraceWidth * trace_cap), 0, s))) return e;
-    // 2 per block of the largest grid, 1 per chunk
-    if ((e = ctx->tr_part.reserve((size_t)(2 * 8 * ctx->num_sms * 8 + nchunks + 1), 0, s))) return e;
+    // 2 per block of the largest grid, 1 per chunk (the planar chunks are the smaller)
+    if ((e = ctx->tr_part.reserve((size_t)(2 * 8 * ctx->num_sms * 8 + planar_chunks(m) + 1), 0, s))) return e;
   }
-  a.trace = tracing ? (ctx->params.log_bbpgd_trace == 2 ? 2 : 1) : 0;
-  a.tr_part = ctx->tr_part.p;
-  a.trace_out = ctx->trace_dev.p;
-  a.trace_cap = trace_cap;
+  const int trace = tracing ? (ctx->params.log_bbpgd_trace == 2 ? 2 : 1) : 0;
 
   // out-of-plane Brownian kicks (-monolayer off) leave the planar form
   const bool planar = ctx->planar && ctx->params.solver_variant != PCC_SOLVER_GENERAL &&
                       !(ctx->uext_active && !ctx->params.monolayer);
   const bool mixed = planar && ctx->params.precision == PCC_PRECISION_MIXED;
-  PlanarArgs<double> pa;
-  PlanarArgs<float> pf;
-  if (planar) {
-    const size_t ne = 2 * m;
-    if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_st0.reserve(mm, 0, s)) || (e = ctx->p_st1.reserve(mm, 0, s)))
+  int kind = 0;
+  if (planar) {  // records ev[0] itself, after packing its operands
+    const PlanarTrace tr{trace, ctx->tr_part.p, ctx->trace_dev.p, trace_cap};
+    e = planar_bbpgd(ctx, dt, mixed, tr, &kind);
+  } else {
+    if ((e = ctx->gam_a.reserve(mm, 0, s)) || (e = ctx->gam_b.reserve(mm, 0, s)) || (e = ctx->g_a.reserve(mm, 0, s)) ||
+        (e = ctx->g_b.reserve(mm, 0, s)))
       return e;
-    if (mixed) {
-      if ((e = ctx->pf_n.reserve(mm, 0, s)) || (e = ctx->pf_t.reserve(mm, 0, s)) || (e = ctx->pf_s.reserve(mm, 0, s)) ||
-          (e = ctx->pf_inc.reserve(ne + 1, 0, s)) || (e = ctx->pf_cell.reserve(nn, 0, s)) ||
-          (e = ctx->pf_u.reserve(nn, 0, s)))
-        return e;
-    } else {
-      if ((e = ctx->p_n.reserve(mm, 0, s)) || (e = ctx->p_t.reserve(mm, 0, s)) || (e = ctx->p_s.reserve(mm, 0, s)) ||
-          (e = ctx->p_inc.reserve(ne + 1, 0, s)) || (e = ctx->p_cell.reserve(nn, 0, s)) ||
-          (e = ctx->p_u.reserve(nn, 0, s)))
-        return e;
+    if ((e = ctx->partials.reserve(4 * (nchunks + 1), 0, s))) return e;
+    SolverArgs a;
+    ConsView cv = ctx->cons.view();
+    a.m = (long long)m;
+    a.gi = cv.gi;
+    a.gj = cv.gj;
+    a.nx = cv.nx;
+    a.ny = cv.ny;
+    a.nz = cv.nz;
+    a.tix = cv.tix;
+    a.tiy = cv.tiy;
+    a.tiz = cv.tiz;
+    a.tjx = cv.tjx;
+    a.tjy = cv.tjy;
+    a.tjz = cv.tjz;
+    a.si = cv.si;
+    a.sj = cv.sj;
+    a.phi = cv.sd;
+    a.gamma = cv.gamma;
+    a.gam[0] = ctx->gam_a.p;
+    a.gam[1] = ctx->gam_b.p;
+    a.g[0] = ctx->g_a.p;
+    a.g[1] = ctx->g_b.p;
+    a.n = (long long)n;
+    a.inc_off = ctx->inc_off.p;
+    a.inc_ent = ctx->inc_ent.p;
+    a.Mlin = ctx->Mlin.p;
+    a.Mrot = ctx->Mrot.p;
+    a.len = ctx->cells.len.p;
+    a.ldot_prev = ctx->cells.ldot.p;
+    a.uext = ctx->uext_active ? ctx->uext.p : nullptr;
+    a.U = ctx->U.p;
+    a.dl = ctx->dldot.p;
+    a.F = ctx->F.p;
+    a.sig = ctx->sig.p;
+    a.ldot = ctx->ldot_new.p;
+    a.imp = ctx->imp_new.p;
+    a.dt = dt;
+    a.lambda = ctx->params.lambda;
+    a.tau = ctx->params.tau;
+    a.tol = ctx->params.tolerance;
+    a.max_it = ctx->params.max_bbpgd_iterations;
+    a.partials = ctx->partials.p;
+    a.nchunks = nchunks;
+    a.sc = ctx->scal.p;
+    a.st = ctx->status;
+    a.trace = trace;
+    a.tr_part = ctx->tr_part.p;
+    a.trace_out = ctx->trace_dev.p;
+    a.trace_cap = trace_cap;
+    const void* kern = tracing ? (const void*)k_bbpgd<1> : (const void*)k_bbpgd<0>;
+    int& coop = ctx->coop_blocks;
+    if (coop == 0) {
+      int per_sm = 0;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0))) return e;
+      // at most 4 blocks per SM: the two grid barriers of every iteration cost
+      // more with more arriving blocks than the extra resident warps hide
+      coop = (per_sm < 4 ? per_sm : 4) * ctx->num_sms;
     }
-    if (m) {
-      if (mixed) {
-        k_pack_planar_cons<float><<<grid_for((long long)m), kBlock, 0, s>>>(
-            cv, (long long)m, ctx->p_ij.p, ctx->pf_n.p, ctx->pf_t.p, ctx->pf_s.p, ctx->p_st0.p);
-        k_pack_planar_inc<float><<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne,
-                                                                             ctx->pf_inc.p);
-      } else {
-        k_pack_planar_cons<double><<<grid_for((long long)m), kBlock, 0, s>>>(
-            cv, (long long)m, ctx->p_ij.p, ctx->p_n.p, ctx->p_t.p, ctx->p_s.p, ctx->p_st0.p);
-        k_pack_planar_inc<double><<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne,
-                                                                              ctx->p_inc.p);
-      }
-      ctx->launches += 2;
-    }
-    if (n) {
-      if (mixed)
-        k_pack_planar_cells<float><<<grid_for((long long)n), kBlock, 0, s>>>(
-            ctx->Mlin.p, ctx->Mrot.p, ctx->cells.len.p, ctx->cells.ldot.p, (long long)n, ctx->pf_cell.p);
-      else
-        k_pack_planar_cells<double><<<grid_for((long long)n), kBlock, 0, s>>>(
-            ctx->Mlin.p, ctx->Mrot.p, ctx->cells.len.p, ctx->cells.ldot.p, (long long)n, ctx->p_cell.p);
-      ctx->launches++;
-    }
-    auto fill = [&](auto& q) {
-      q.m = (long long)m;
-      q.n = (long long)n;
-      q.ij = ctx->p_ij.p;
-      q.phi = cv.sd;
-      q.gamma = cv.gamma;
-      q.st[0] = ctx->p_st0.p;
-      q.st[1] = ctx->p_st1.p;
-      q.inc_off = ctx->inc_off.p;
-      q.inc_ent = ctx->inc_ent.p;
-      q.uext = a.uext;
-      q.U = ctx->U.p;
-      q.F = ctx->F.p;
-      q.sig = ctx->sig.p;
-      q.ldot = ctx->ldot_new.p;
-      q.imp = ctx->imp_new.p;
-      q.dt = dt;
-      q.lambda = ctx->params.lambda;
-      q.tau = ctx->params.tau;
-      q.tol = ctx->params.tolerance;
-      q.max_it = ctx->params.max_bbpgd_iterations;
-      q.partials = ctx->partials.p;
-      q.nchunks = nchunks;
-      q.sc = ctx->scal.p;
-      q.st_err = ctx->status;
-      q.trace = a.trace;
-      q.tr_part = a.tr_part;
-      q.trace_out = a.trace_out;
-      q.trace_cap = a.trace_cap;
-    };
-    fill(pa);
-    fill(pf);
-    pa.nn = ctx->p_n.p;
-    pa.tt = ctx->p_t.p;
-    pa.ss = ctx->p_s.p;
-    pa.inc = ctx->p_inc.p;
-    pa.cell = ctx->p_cell.p;
-    pa.u = ctx->p_u.p;
-    pf.nn = ctx->pf_n.p;
-    pf.tt = ctx->pf_t.p;
-    pf.ss = ctx->pf_s.p;
-    pf.inc = ctx->pf_inc.p;
-    pf.cell = ctx->pf_cell.p;
-    pf.u = ctx->pf_u.p;
+    long long want = (long long)grid_for((long long)n);
+    if (nchunks > want) want = nchunks;
+    if (want > coop) want = coop;
+    // Small colonies run in one block: its barriers are block barriers, it
+    // needs no co-residency guarantee, so it is an ordinary launch that runs
+    // beside other colonies' kernels.  The result does not depend on the grid.
+    if (n <= (size_t)kOneBlockCells && m <= (size_t)kOneBlockConstraints) want = 1;
+    if (want < 1) want = 1;
+    void* args[] = {&a};
+    if (ctx->profiling) cudaEventRecord(ctx->ev[0], s);
+    if (want == 1)
+      e = cudaLaunchKernel(kern, dim3(1), dim3(kBlock), args, 0, s);
+    else
+      e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)want), dim3(kBlock), args, 0, s);
+    kind = want > 1 ? 1 : 0;
   }
-  // small planar colonies without a trace: the one-CTA kernel (same values)
-  const bool small = planar && !tracing && n <= (size_t)kSmallCells && m <= (size_t)kSmallConstraints;
-  const void* kern;
-  if (small)
-    kern = mixed ? (const void*)k_bbpgd_planar_small<float> : (const void*)k_bbpgd_planar_small<double>;
-  else if (tracing)
-    kern = mixed ? (const void*)k_bbpgd_planar<float, 1>
-                 : planar ? (const void*)k_bbpgd_planar<double, 1> : (const void*)k_bbpgd<1>;
-  else
-    kern = mixed ? (const void*)k_bbpgd_planar<float, 0>
-                 : planar ? (const void*)k_bbpgd_planar<double, 0> : (const void*)k_bbpgd<0>;
-  int& coop = mixed ? ctx->coop_blocks_mixed : planar ? ctx->coop_blocks_planar : ctx->coop_blocks;
-  if (coop == 0 && !small) {
-    int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0))) return e;
-    // at most 4 blocks per SM: the two grid barriers of every iteration cost
-    // more with more arriving blocks than the extra resident warps hide
-    coop = (per_sm < 4 ? per_sm : 4) * ctx->num_sms;
-  }
-  long long want = (long long)grid_for((long long)n);
-  if (nchunks > want) want = nchunks;
-  if (want > coop) want = coop;
-  // Small colonies run in one block: its barriers are block barriers, it
-  // needs no co-residency guarantee, so it is an ordinary launch that runs
-  // beside other colonies' kernels.  The result does not depend on the grid.
-  if (n <= (size_t)kOneBlockCells && m <= (size_t)kOneBlockConstraints) want = 1;
-  if (want < 1) want = 1;
-  void* args[] = {mixed ? (void*)&pf : planar ? (void*)&pa : (void*)&a};
-  if (ctx->profiling) cudaEventRecord(ctx->ev[0], s);
-  if (small)
-    e = cudaLaunchKernel(kern, dim3(1), dim3(kSmallThreads), args, 0, s);
-  else if (want == 1)
-    e = cudaLaunchKernel(kern, dim3(1), dim3(kBlock), args, 0, s);
-  else
-    e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)want), dim3(kBlock), args, 0, s);
-  if (small || want == 1)
-    ctx->prof.bbpgd_cta_launches++;
-  else
-    ctx->prof.bbpgd_grid_launches++;
   ctx->launches++;
   if (e) return e;
+  if (kind)
+    ctx->prof.bbpgd_grid_launches++;
+  else
+    ctx->prof.bbpgd_cta_launches++;
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);
   SolverScalars host;
   if ((e = cudaMemcpyAsync(&host, ctx->scal.p, sizeof host, cudaMemcpyDeviceToHost, s))) return e;
