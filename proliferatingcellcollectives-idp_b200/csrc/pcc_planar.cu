@@ -44,14 +44,9 @@ namespace pcc {
 
 namespace {
 
-constexpr int kPChunk = kBlock;            // constraints per reduction chunk: one per thread of a unit
-constexpr int kLanes = 4;                  // lanes per cell in the cell pass
-constexpr int kCtaThreads = 4 * kBlock;    // one-CTA form: four 256-thread units
-constexpr int kCtaUnits = kCtaThreads / kBlock;
 constexpr int kCtaCells = 1024;            // the one-CTA form up to this many cells ...
 constexpr int kCtaConstraints = 4096;      // ... and constraints
 constexpr int kMaxBlocksPerSm = 4;        // co-resident blocks per SM of the multi-block form
-constexpr unsigned kFull = 0xffffffffu;
 
 template <class Real>
 struct PT;
@@ -121,62 +116,6 @@ struct PArgs {
   double* trace_out;
   long long trace_cap;
 };
-
-// Work units.  A unit is 256 threads; chunk ch belongs to unit ch % units.
-struct GridUnits {  // the multi-block kernel: one unit per block
-  __device__ static unsigned units() { return gridDim.x; }
-  __device__ static unsigned unit() { return blockIdx.x; }
-  __device__ static int t() { return threadIdx.x; }
-  __device__ static void sync() { __syncthreads(); }
-  __device__ static long long warp() { return ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
-  __device__ static long long warps() { return ((long long)gridDim.x * blockDim.x) >> 5; }
-};
-struct CtaUnits {  // the one-CTA kernel: four units in one block, each with its own named barrier
-  __device__ static unsigned units() { return kCtaUnits; }
-  __device__ static unsigned unit() { return threadIdx.x / kBlock; }
-  __device__ static int t() { return threadIdx.x % kBlock; }
-  __device__ static void sync() { asm volatile("bar.sync %0, %1;" ::"r"(unit() + 1), "r"(kBlock) : "memory"); }
-  __device__ static long long warp() { return threadIdx.x >> 5; }
-  __device__ static long long warps() { return kCtaThreads / 32; }
-};
-
-// (sum, sum, sum, max) over a warp by an xor tree (every lane ends with the same bits).
-__device__ __forceinline__ void warp_reduce4(double v[4]) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    v[0] = add(v[0], __shfl_xor_sync(kFull, v[0], o));
-    v[1] = add(v[1], __shfl_xor_sync(kFull, v[1], o));
-    v[2] = add(v[2], __shfl_xor_sync(kFull, v[2], o));
-    const double y = __shfl_xor_sync(kFull, v[3], o);
-    v[3] = v[3] < y ? y : v[3];
-  }
-}
-
-// A unit's 256 values into thread 0 of the unit: the warp tree, then an xor
-// tree over the unit's 8 warp results.  sm: 32 doubles of this unit.
-template <class U>
-__device__ __forceinline__ void unit_reduce4(double v[4], double* sm) {
-  warp_reduce4(v);
-  const int t = U::t(), lane = t & 31, w = t >> 5;
-  if (lane == 0) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) sm[4 * w + q] = v[q];
-  }
-  U::sync();
-  if (w == 0) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) v[q] = lane < kBlock / 32 ? sm[4 * lane + q] : 0.0;
-#pragma unroll
-    for (int o = kBlock / 64; o > 0; o >>= 1) {
-      v[0] = add(v[0], __shfl_xor_sync(kFull, v[0], o));
-      v[1] = add(v[1], __shfl_xor_sync(kFull, v[1], o));
-      v[2] = add(v[2], __shfl_xor_sync(kFull, v[2], o));
-      const double y = __shfl_xor_sync(kFull, v[3], o);
-      v[3] = v[3] < y ? y : v[3];
-    }
-  }
-  U::sync();  // sm is reused by the next call
-}
 
 __device__ __forceinline__ double lane_add(double a, double b) { return add(a, b); }
 __device__ __forceinline__ float lane_add(float a, float b) { return __fadd_rn(a, b); }
@@ -359,20 +298,6 @@ __device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, 
       }
     }
   }
-}
-
-// Sum of the chunk partials by one unit (thread t takes chunks t, t + 256, ...).
-template <class U>
-__device__ __forceinline__ void reduce_partials(const double4* partials, long long nchunks, double v[4], double* sm) {
-  v[0] = v[1] = v[2] = v[3] = 0.0;
-  for (long long ch = U::t(); ch < nchunks; ch += kBlock) {
-    const double4 q = ldcg(partials + ch);
-    v[0] = add(v[0], q.x);
-    v[1] = add(v[1], q.y);
-    v[2] = add(v[2], q.z);
-    v[3] = v[3] < q.w ? q.w : v[3];
-  }
-  unit_reduce4<U>(v, sm);
 }
 
 __device__ __forceinline__ void trace_cells(double* smt, double eq, double eg, double* tr_part) {

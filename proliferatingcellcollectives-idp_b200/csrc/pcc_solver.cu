@@ -1,20 +1,26 @@
-// Hard-model BBPGD solver and soft-model force assembly (sm_100a).
+// Hard-model BBPGD solver for non-planar colonies, the per-step solver glue
+// and the soft-model force assembly (sm_100a).
 //
 // The BBPGD solve (solver/BBPGD.cpp:32-127 with the gradient of
 // dynamics/models/hard/HardModelGradient.cpp:89-158) runs as ONE persistent
 // cooperative kernel per ReLCP phase.  Each iteration is two grid-wide passes:
-//   pass A, one thread per cell: F = D^T (gamma - gamma_old) and
-//     sigma = L^T gamma gathered over the cell's incidence list (ascending
-//     constraint order, no atomics), U = M F, growth rate and its change;
-//   pass B, one thread per constraint: phi_next = Phi + dt D U - dt L dldot,
-//     the projected-gradient residual and the three Barzilai-Borwein dot
-//     products, reduced per fixed chunk of constraints.
+//   cell pass, kLanes lanes per cell: F = D^T (gamma - gamma_old) and
+//     sigma = L^T gamma over the cell's incidence list (lane l takes entries
+//     l, l + kLanes, ... in ascending constraint order; the lanes' sums meet
+//     in a fixed shuffle tree; no atomics), U = M F, growth rate and its change;
+//   constraint pass, one thread per constraint: phi_next = Phi + dt D U -
+//     dt L dldot, the projected-gradient residual and the three
+//     Barzilai-Borwein dot products, reduced per fixed chunk of kPChunk
+//     constraints.
 // The projection gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0) is recomputed
 // where it is needed (both passes), so no extra pass stores it.  The last block
 // to reach a barrier reduces the chunk partials in a fixed order and publishes
 // alpha and the convergence decision: results do not depend on the grid size
-// or on which block arrives last.  Barrier waits are bounded; a wait that runs
-// out raises kDevErrTimeout and the kernel returns.
+// or on which block arrives last.  The decomposition and every reduction tree
+// are those of the planar kernels (pcc_planar.cu), which skip only exact
+// zeros, so a planar colony gives the same bits on either path.  Barrier
+// waits are bounded; a wait that runs out raises kDevErrTimeout and the
+// kernel returns.
 #include <cfloat>
 #include <cmath>
 
@@ -25,11 +31,6 @@ namespace pcc {
 
 namespace {
 
-constexpr int kChunk = 1024;            // constraints per reduction chunk
-constexpr int kPerThread = kChunk / kBlock;
-// A measured colony of 1,309 cells iterated faster over several SMs than in
-// one 1024-thread CTA, so the one-CTA form stops where one block would
-// otherwise hold the whole colony anyway.
 constexpr int kOneBlockCells = 1024;      // otherwise one 256-thread block up to this many cells ...
 constexpr int kOneBlockConstraints = 4096;  // ... and constraints
 
@@ -64,69 +65,89 @@ struct SolverArgs {
 
 
 
-// Pass A for cell p.  mode 0: gamma = gamma_0; mode 1: gamma_k projected from
+// Cell pass.  mode 0: gamma = gamma_0; mode 1: gamma_k projected from
 // (gam_prev, g_prev, alpha).  Writes U and dldot; with `final` also F, sigma,
 // ldot and impedance.
-__device__ __forceinline__ void cell_pass(const SolverArgs& a, long long p, int mode, const double* gprev_gam,
-                                          const double* gprev_g, double alpha, bool final, double* eq = nullptr,
-                                          double* eg = nullptr) {
-  double F[6] = {0, 0, 0, 0, 0, 0};
-  double Fg[6] = {0, 0, 0, 0, 0, 0};  // D^T gamma (trace only)
-  double sg = 0.0;
-  const int b = a.inc_off[p], e = a.inc_off[p + 1];
-  for (int k = b; k < e; ++k) {
-    const int ent = a.inc_ent[k];
-    const long long c = ent >> 1;
-    const int side = ent & 1;
-    const double gold = a.gamma[c];
-    const double gc = mode == 0 ? gold : project(ldcg(gprev_gam + c), ldcg(gprev_g + c), alpha);
-    const double diff = sub(gc, gold);
-    double D[6];
-    if (side == 0) {
-      D[0] = a.nx[c];
-      D[1] = a.ny[c];
-      D[2] = a.nz[c];
-      D[3] = a.tix[c];
-      D[4] = a.tiy[c];
-      D[5] = a.tiz[c];
-    } else {
-      D[0] = -a.nx[c];
-      D[1] = -a.ny[c];
-      D[2] = -a.nz[c];
-      D[3] = a.tjx[c];
-      D[4] = a.tjy[c];
-      D[5] = a.tjz[c];
+template <int kTr>
+__device__ __forceinline__ void cell_pass(const SolverArgs& a, int mode, const double* gprev_gam,
+                                          const double* gprev_g, double alpha, bool final, double* eq, double* eg) {
+  const int lane = threadIdx.x & 31, gl = lane % kLanes;
+  constexpr long long kCellsPerWarp = 32 / kLanes;
+  for (long long pw = GridUnits::warp() * kCellsPerWarp; pw < a.n; pw += GridUnits::warps() * kCellsPerWarp) {
+    const long long p = pw + lane / kLanes;
+    int b = 0, e = 0;
+    if (p < a.n) {
+      b = a.inc_off[p];
+      e = a.inc_off[p + 1];
+    }
+    double F[6] = {0, 0, 0, 0, 0, 0};
+    double Fg[6] = {0, 0, 0, 0, 0, 0};  // D^T gamma (trace only)
+    double sg = 0.0;
+    for (int k = b + gl; k < e; k += kLanes) {
+      const int ent = a.inc_ent[k];
+      const long long c = ent >> 1;
+      const int side = ent & 1;
+      const double gold = a.gamma[c];
+      const double gc = mode == 0 ? gold : project(ldcg(gprev_gam + c), ldcg(gprev_g + c), alpha);
+      const double diff = sub(gc, gold);
+      double D[6];
+      if (side == 0) {
+        D[0] = a.nx[c];
+        D[1] = a.ny[c];
+        D[2] = a.nz[c];
+        D[3] = a.tix[c];
+        D[4] = a.tiy[c];
+        D[5] = a.tiz[c];
+      } else {
+        D[0] = -a.nx[c];
+        D[1] = -a.ny[c];
+        D[2] = -a.nz[c];
+        D[3] = a.tjx[c];
+        D[4] = a.tjy[c];
+        D[5] = a.tjz[c];
+      }
+#pragma unroll
+      for (int q = 0; q < 6; ++q) F[q] = add(F[q], mul(D[q], diff));
+      sg = add(sg, mul(side == 0 ? a.si[c] : a.sj[c], gc));
+      if constexpr (kTr) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) Fg[q] = add(Fg[q], mul(D[q], gc));
+      }
     }
 #pragma unroll
-    for (int q = 0; q < 6; ++q) F[q] = add(F[q], mul(D[q], diff));
-    sg = add(sg, mul(side == 0 ? a.si[c] : a.sj[c], gc));
-    if (eq) {
+    for (int o = kLanes / 2; o > 0; o >>= 1) {
 #pragma unroll
-      for (int q = 0; q < 6; ++q) Fg[q] = add(Fg[q], mul(D[q], gc));
+      for (int q = 0; q < 6; ++q) F[q] = add(F[q], __shfl_xor_sync(kFull, F[q], o));
+      sg = add(sg, __shfl_xor_sync(kFull, sg, o));
+      if constexpr (kTr) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) Fg[q] = add(Fg[q], __shfl_xor_sync(kFull, Fg[q], o));
+      }
     }
-  }
-  const double ml = a.Mlin[p], mr = a.Mrot[p];
-  double* U = a.U + 6 * p;
+    if (gl != 0 || p >= a.n) continue;
+    const double ml = a.Mlin[p], mr = a.Mrot[p];
+    double* U = a.U + 6 * p;
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    const double uc = add(0.0, mul(q < 3 ? ml : mr, F[q]));
-    // U = U_ext + M F (VecWAXPY, HardModelGradient.cpp:21); U_ext is rotational only
-    U[q] = add(uc, (q >= 3 && a.uext) ? a.uext[3 * p + q - 3] : 0.0);
-  }
-  double im = exp(vscale(-a.lambda, sg));
-  double ld = vscale(dvd(1.0, a.tau), mul(a.len[p], im));
-  a.dl[p] = sub(ld, a.ldot_prev[p]);
-  if (eq) {
+    for (int q = 0; q < 6; ++q) {
+      const double uc = add(0.0, mul(q < 3 ? ml : mr, F[q]));
+      // U = U_ext + M F (VecWAXPY, HardModelGradient.cpp:21); U_ext is rotational only
+      U[q] = add(uc, (q >= 3 && a.uext) ? a.uext[3 * p + q - 3] : 0.0);
+    }
+    const double im = exp(vscale(-a.lambda, sg));
+    const double ld = vscale(dvd(1.0, a.tau), mul(a.len[p], im));
+    a.dl[p] = sub(ld, a.ldot_prev[p]);
+    if constexpr (kTr) {
 #pragma unroll
-    for (int q = 0; q < 6; ++q) *eq = add(*eq, mul(Fg[q], mul(q < 3 ? ml : mr, Fg[q])));
-    *eg = add(*eg, mul(a.len[p], im));
-  }
-  if (final) {
+      for (int q = 0; q < 6; ++q) *eq = add(*eq, mul(Fg[q], mul(q < 3 ? ml : mr, Fg[q])));
+      *eg = add(*eg, mul(a.len[p], im));
+    }
+    if (final) {
 #pragma unroll
-    for (int q = 0; q < 6; ++q) a.F[6 * p + q] = F[q];
-    a.sig[p] = sg;
-    a.ldot[p] = ld;
-    a.imp[p] = im;
+      for (int q = 0; q < 6; ++q) a.F[6 * p + q] = F[q];
+      a.sig[p] = sg;
+      a.ldot[p] = ld;
+      a.imp[p] = im;
+    }
   }
 }
 
@@ -178,49 +199,64 @@ __device__ __forceinline__ void trace_chunk(double* sm, double lin, double* tr_p
   if (threadIdx.x == 0) tr_part[2 * nb + ch] = v[0];
 }
 
+// Constraint pass over the chunks of this block: new (gamma, g) into
+// (gam_out, g_out) and the chunk partials; mode 0 evaluates g at gamma_0
+// (residual only).
+template <int kTr>
+__device__ __forceinline__ void constraint_pass(const SolverArgs& a, int mode, const double* gp, const double* gg,
+                                                double* gam_out, double* g_out, double alpha, bool check, double* sm,
+                                                double* smt) {
+  double4* partials = reinterpret_cast<double4*>(a.partials);
+  for (long long ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+    double v[4] = {0, 0, 0, 0};  // sum dgam^2, sum dgam*dg, sum dg^2, max residual
+    double lin = 0.0;
+    const long long c = ch * kPChunk + threadIdx.x;
+    if (c < a.m) {
+      const double gpc = mode == 0 ? a.gamma[c] : ldcg(gp + c), ggc = mode == 0 ? 0.0 : ldcg(gg + c);
+      const double gam = mode == 0 ? gpc : project(gpc, ggc, alpha);
+      const double g = constraint_grad(a, c);
+      gam_out[c] = gam;
+      g_out[c] = g;
+      if (mode != 0) {
+        const double dgm = sub(gam, gpc), dg = sub(g, ggc);
+        v[0] = mul(dgm, dgm);
+        v[1] = mul(dgm, dg);
+        v[2] = mul(dg, dg);
+      }
+      if (mode == 0 || check) v[3] = proj_grad_abs(g, gam);
+      if constexpr (kTr) lin = mul(gam, a.phi[c]);
+    }
+    unit_reduce4<GridUnits>(v, sm);
+    if (threadIdx.x == 0) partials[ch] = make_double4(v[0], v[1], v[2], v[3]);
+    if constexpr (kTr) {
+      if (a.trace) trace_chunk(smt, lin, a.tr_part, gridDim.x, ch);
+    }
+  }
+}
+
 // kTr = 1 compiles the trace hooks in; the untraced kernel carries none of them.
 template <int kTr>
 __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   const int TR = kTr ? a.trace : 0;
-  __shared__ double sm[4 * kBlock];
+  __shared__ double sm[4 * (kBlock / 32)];
+  __shared__ double smt[kTr ? 4 * kBlock : 1];
   const unsigned nb = gridDim.x;
   const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
   const long long stride = (long long)nb * kBlock;
   SolverScalars* sc = a.sc;
+  const double4* partials = reinterpret_cast<const double4*>(a.partials);
 
   // ---- gradient at gamma_0 and the initial residual (BBPGD.cpp:40-44)
   {
     double eq = 0.0, eg = 0.0;
-    for (long long p = tid; p < a.n; p += stride)
-      cell_pass(a, p, 0, nullptr, nullptr, 0.0, false, TR ? &eq : nullptr, &eg);
-    if (TR) trace_cells(sm, eq, eg, a.tr_part);
+    cell_pass<kTr>(a, 0, nullptr, nullptr, 0.0, false, &eq, &eg);
+    if (TR) trace_cells(smt, eq, eg, a.tr_part);
   }
   if (!barrier(sc, nb, a.st)) return;
-  for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
-    double v[4] = {0, 0, 0, 0};
-    double lin = 0.0;
-    for (int k = 0; k < kPerThread; ++k) {
-      long long c = ch * kChunk + k * kBlock + threadIdx.x;
-      if (c >= a.m) break;
-      double g = constraint_grad(a, c);
-      double gm = a.gamma[c];
-      a.g[0][c] = g;
-      a.gam[0][c] = gm;
-      double r = proj_grad_abs(g, gm);
-      v[3] = v[3] < r ? r : v[3];
-      if (TR) lin = add(lin, mul(gm, a.phi[c]));
-    }
-    block_reduce4(v, sm);
-    if (threadIdx.x == 0) a.partials[4 * ch + 3] = v[3];
-    if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
-  }
+  constraint_pass<kTr>(a, 0, nullptr, nullptr, a.gam[0], a.g[0], 0.0, true, sm, smt);
   auto reduce_init = [&]() {
-    double v[4] = {0, 0, 0, 0};
-    for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
-      double r = ldcg(a.partials + 4 * ch + 3);
-      v[3] = v[3] < r ? r : v[3];
-    }
-    block_reduce4(v, sm);
+    double v[4];
+    reduce_partials<GridUnits>(partials, a.nchunks, v, sm);
     if (threadIdx.x == 0) {
       sc->res0 = v[3];
       sc->residual = v[3];
@@ -228,7 +264,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
       sc->converged = 0;
     }
     if (TR)
-      trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
+      trace_record(smt, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
                    a.trace_cap);
   };
   if (!barrier_reduce(sc, nb, a.st, reduce_init)) return;
@@ -239,59 +275,18 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
     const double alpha = *(volatile double*)&sc->alpha;
     // with the trace on the residual is evaluated (and tested) every iteration (BBPGD.cpp:73)
     const bool check = (it % 10) == 0 || TR;
-    const double* gp = a.gam[p];
-    const double* gg = a.g[p];
-    double* gc_out = a.gam[1 - p];
-    double* g_out = a.g[1 - p];
     {
       double eq = 0.0, eg = 0.0;
-      for (long long q = tid; q < a.n; q += stride)
-        cell_pass(a, q, 1, gp, gg, alpha, check, TR ? &eq : nullptr, &eg);
-      if (TR) trace_cells(sm, eq, eg, a.tr_part);
+      cell_pass<kTr>(a, 1, a.gam[p], a.g[p], alpha, check, &eq, &eg);
+      if (TR) trace_cells(smt, eq, eg, a.tr_part);
     }
     if (!barrier(sc, nb, a.st)) return;
-    for (long long ch = blockIdx.x; ch < a.nchunks; ch += nb) {
-      double v[4] = {0, 0, 0, 0};  // sum dgam^2, sum dgam*dg, sum dg^2, max residual
-      double lin = 0.0;
-      for (int k = 0; k < kPerThread; ++k) {
-        long long c = ch * kChunk + k * kBlock + threadIdx.x;
-        if (c >= a.m) break;
-        const double gpc = ldcg(gp + c), ggc = ldcg(gg + c);
-        const double gam = project(gpc, ggc, alpha);
-        const double g = constraint_grad(a, c);
-        gc_out[c] = gam;
-        g_out[c] = g;
-        const double dgm = sub(gam, gpc), dg = sub(g, ggc);
-        v[0] = add(v[0], mul(dgm, dgm));
-        v[1] = add(v[1], mul(dgm, dg));
-        v[2] = add(v[2], mul(dg, dg));
-        if (check) {
-          double r = proj_grad_abs(g, gam);
-          v[3] = v[3] < r ? r : v[3];
-        }
-        if (TR) lin = add(lin, mul(gam, a.phi[c]));
-      }
-      block_reduce4(v, sm);
-      if (threadIdx.x == 0) {
-        a.partials[4 * ch + 0] = v[0];
-        a.partials[4 * ch + 1] = v[1];
-        a.partials[4 * ch + 2] = v[2];
-        a.partials[4 * ch + 3] = v[3];
-      }
-      if (TR) trace_chunk(sm, lin, a.tr_part, nb, ch);
-    }
+    constraint_pass<kTr>(a, 1, a.gam[p], a.g[p], a.gam[1 - p], a.g[1 - p], alpha, check, sm, smt);
     auto reduce_iter = [&]() {
-      double v[4] = {0, 0, 0, 0};
-      for (long long ch = threadIdx.x; ch < a.nchunks; ch += kBlock) {
-        v[0] = add(v[0], ldcg(a.partials + 4 * ch + 0));
-        v[1] = add(v[1], ldcg(a.partials + 4 * ch + 1));
-        v[2] = add(v[2], ldcg(a.partials + 4 * ch + 2));
-        double r = ldcg(a.partials + 4 * ch + 3);
-        v[3] = v[3] < r ? r : v[3];
-      }
-      block_reduce4(v, sm);
+      double v[4];
+      reduce_partials<GridUnits>(partials, a.nchunks, v, sm);
       if (TR)
-        trace_record(sm, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, it, v[3], alpha, a.trace_out,
+        trace_record(smt, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, it, v[3], alpha, a.trace_out,
                      a.trace_cap);
       if (threadIdx.x == 0) {
         int conv = 0;
@@ -573,7 +568,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     return e;
   if ((e = ctx->scal.reserve(1, 0, s))) return e;
   cudaMemsetAsync(ctx->scal.p, 0, sizeof(SolverScalars), s);
-  const long long nchunks = (long long)((m + kChunk - 1) / kChunk);
+  const long long nchunks = planar_chunks(m);  // kPChunk constraints per chunk, as the planar kernels
   const bool tracing = ctx->trace_active;
   long long trace_cap = 0;
   if (tracing) {
@@ -656,7 +651,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
       // more with more arriving blocks than the extra resident warps hide
       coop = (per_sm < 4 ? per_sm : 4) * ctx->num_sms;
     }
-    long long want = (long long)grid_for((long long)n);
+    long long want = (long long)grid_for((long long)n * kLanes);
     if (nchunks > want) want = nchunks;
     if (want > coop) want = coop;
     // Small colonies run in one block: its barriers are block barriers, it
