@@ -18,8 +18,15 @@ import numpy as np
 
 
 def dense_colony(radius: float, seed: int = 0, l0: float = 1.0, patch: float = 12.0, lane_gap: float = 0.01,
-                 end_gap: float = 0.02) -> dict:
+                 end_gap: float = 0.02, angle_jitter: float = 1e-6) -> dict:
+    """Cells of one patch share the patch orientation up to a uniform jitter of
+    +-angle_jitter radians per cell.  Exactly parallel neighbours make the
+    segment-distance determinant a*c - b^2 pure rounding noise, so their
+    closest points (and the reference's, which take the pair in hash-map
+    order) depend on the order the two segments are taken in; the jitter keeps
+    every pair away from that case."""
     rng = np.random.default_rng(seed)
+    jit = np.random.default_rng(seed + 7919)
     d = l0 / 2
     xs, ys, ths, ls = [], [], [], []
     n_p = int(np.ceil(radius / patch)) + 1
@@ -52,7 +59,7 @@ def dense_colony(radius: float, seed: int = 0, l0: float = 1.0, patch: float = 1
                     if inside_patch and inside_disc:
                         xs.append(c[0])
                         ys.append(c[1])
-                        ths.append(th)
+                        ths.append(th + jit.uniform(-angle_jitter, angle_jitter))
                         ls.append(L)
                     s += L + end_gap
                 lane += d + lane_gap

@@ -195,6 +195,25 @@ def dense_fixture(name: str, radius: float, seed: int, cont_steps: int, lists=("
     print(name, len(cells["x"]), "cells", out["det25_sd"].size, "phase-0 contacts")
 
 
+def tight_fixture(name: str, source: str, prefix: str, tolerance: float):
+    """One reference solver call at a tight tolerance on a snapshot of another
+    fixture: both solvers then converge to the same LCP solution, which pins
+    the device's solve beyond the 1e-3 tolerance at which two valid solutions
+    may differ by about the tolerance."""
+    src = np.load(OUT / f"{source}.npz", allow_pickle=True)
+    snap = {k[len(f"{prefix}cells_"):]: src[k] for k in src.files if k.startswith(f"{prefix}cells_")}
+    p = abi.default_params()
+    for k, v in src["params"][0].items():
+        setattr(p, k, v)
+    p.tolerance = tolerance
+    dt = float(src[f"{prefix}dt"])
+    out: dict = {"params": np.array([params_dict(p)], dtype=object), "dt": np.array(dt)}
+    pack("cells_", snap, out)
+    one_solve(p, snap, dt, out, "solve_", light=True)
+    np.savez_compressed(OUT / f"{name}.npz", **out)
+    print(name, len(snap["x"]), "cells", out["solve_stats"][0])
+
+
 def soft_grown_fixture(name: str, p: abi.Params, radius: float):
     """A soft-model colony grown by the reference from one cell to `radius`
     (the cell-count history of every step, the radius every 1000 steps, the
@@ -295,6 +314,8 @@ FIXTURES = {
         "grown_soft_r20_seed0", abi.default_params(dt=3e-5, fixed_dt=1, seed=0, mode=abi.MODE_SOFT,
                                                    ghost_mode=abi.GHOSTS_SINGLE_RANK, kcc=1333.3333333333333), 20.0),
     "brownian_r10_seed3": lambda: brownian_fixture("brownian_r10_seed3"),
+    # the 1,100-cell snapshot of grown_hard_r20_seed0 solved at tolerance 1e-6
+    "grown_hard_r20_tight": lambda: tight_fixture("grown_hard_r20_tight", "grown_hard_r20_seed0", "mid_", 1e-6),
 }
 
 
