@@ -15,10 +15,25 @@ constexpr long long kSpinLimit = 1LL << 26;
 constexpr int kTraceWidth = 8;  // it, residual, step size, linear, quadratic, growth, total, -
 // Work decomposition shared by the general and planar solvers (identical
 // values from both): kLanes lanes per cell in the cell pass (lane l takes
-// the cell's incidence entries l, l + kLanes, ...), kPChunk constraints per
-// reduction chunk (one per thread of a 256-thread unit).
-constexpr int kPChunk = kBlock;
+// the cell's incidence entries l, l + kLanes, ...); a reduction chunk is
+// 256 x S constraints, thread t of a 256-thread unit taking constraints
+// t, t + 256, ... of the chunk and summing its S terms in that order before
+// the unit's fixed shuffle tree.  S depends on the constraint count alone:
+// the smallest S (at most kMaxPerThread) that packs the constraints into at
+// most kChunkTarget chunks, one round of a grid of four 256-thread blocks on
+// each of 148 SMs, so every block reduces one chunk per iteration with S
+// independent constraints in flight per thread.  Nothing depends on the grid.
 constexpr int kLanes = 4;
+constexpr long long kChunkTarget = 592;
+constexpr int kMaxPerThread = 8;
+__host__ __device__ inline int chunk_per_thread(long long m) {
+  const long long s = (m + kBlock * kChunkTarget - 1) / (kBlock * kChunkTarget);
+  return s < 1 ? 1 : (s > kMaxPerThread ? kMaxPerThread : (int)s);
+}
+__host__ __device__ inline long long chunk_count(long long m) {
+  const long long per = (long long)kBlock * chunk_per_thread(m);
+  return (m + per - 1) / per;
+}
 constexpr int kCtaThreads = 4 * kBlock;  // one-CTA form: four 256-thread units
 constexpr int kCtaUnits = kCtaThreads / kBlock;
 constexpr unsigned kFull = 0xffffffffu;

@@ -679,7 +679,12 @@ cudaError_t detect_contacts(pcc_ctx* ctx, double tol, int phase, bool reuse, siz
     cudaMemcpyAsync(ctx->pinned_ll + 1, &ctx->status->max_bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                     s);
     cudaMemcpyAsync(pinned + 4, &ctx->status->list_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    // k_bin folds the planarity of the current cells on every pass: cells
+    // that left the plane since the last full pass (out-of-plane Brownian
+    // kicks) must take the general solver
+    cudaMemcpyAsync(pinned + 5, ctx->bbox.p + 6, sizeof(int), cudaMemcpyDeviceToHost, s);
     if ((e = cudaStreamSynchronize(s))) return e;
+    ctx->planar = pinned[5] == 0;
     const unsigned flags = (unsigned)pinned[4];
     if (use_list && (flags & kListStale)) {
       // cells moved too far since the lists were built: rebin this phase

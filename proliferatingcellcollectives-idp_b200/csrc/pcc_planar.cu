@@ -17,8 +17,8 @@
 //     sums of F = D^T (gamma_k - gamma_old) and sigma = L^T gamma_k are combined
 //     by a fixed shuffle tree, and the first lane forms U = M F, the growth
 //     rate and its change;
-//   constraint pass: one thread per constraint in fixed chunks of kPChunk,
-//     phi_next = Phi + dt D U - dt L dldot, the new (gamma_k, g_k) written to
+//   constraint pass: a few constraints per thread in fixed chunks
+//     (chunk_per_thread), phi_next = Phi + dt D U - dt L dldot, the new (gamma_k, g_k) written to
 //     the constraint and pushed to its two incidence entries (so the next
 //     cell pass reads them in order instead of gathering), and the three
 //     Barzilai-Borwein dot products and the residual reduced per chunk by a
@@ -108,6 +108,7 @@ struct PArgs {
   long long max_it;
   double4* partials;       // one per chunk: (sum dgam^2, sum dgam*dg, sum dg^2, max residual)
   long long nchunks;
+  int per_thread;          // constraints per thread in a chunk (chunk_per_thread(m))
   SolverScalars* sc;
   DevStatus* st_err;
   // BBPGD trace (-log_bbgd_trace), as in the general kernel
@@ -120,8 +121,17 @@ struct PArgs {
 __device__ __forceinline__ double lane_add(double a, double b) { return add(a, b); }
 __device__ __forceinline__ float lane_add(float a, float b) { return __fadd_rn(a, b); }
 
+// Lane sums of one cell over its incidence entries.
+template <class Real>
+struct CellAcc {
+  Real f0 = 0, f1 = 0, f5 = 0;
+  double sg = 0.0, g0 = 0.0, g1 = 0.0, g5 = 0.0;
+};
+
 // Cell pass.  mode 0: gamma = gamma_0 (the initial gradient); mode 1: gamma_k
-// projected from the (gamma, g) of buffer `par` with step alpha.
+// projected from the (gamma, g) of buffer `par` with step alpha.  A lane group
+// takes two cells per round (p and p + stride) so the loads of both are in
+// flight together; each cell's sums do not depend on which group takes it.
 template <class Real, class U, int kTr>
 __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, int par, double alpha, bool final,
                                           double* eq, double* eg) {
@@ -130,74 +140,66 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, int pa
   const int lane = threadIdx.x & 31, gl = lane % kLanes;
   constexpr long long kCellsPerWarp = 32 / kLanes;
   const double2* ev = a.ev[par];
-  for (long long pw = U::warp() * kCellsPerWarp; pw < a.n; pw += U::warps() * kCellsPerWarp) {
-    const long long p = pw + lane / kLanes;
-    int b = 0, e = 0;
-    if (p < a.n) {
-      b = a.inc_off[p];
-      e = a.inc_off[p + 1];
+  auto accumulate = [&](CellAcc<Real>& A, int k) {
+    const V4 d = a.inc[k];
+    const double go = a.gold[k];
+    double gc = go;
+    if (mode != 0) {
+      const double2 s = ldcg(ev + k);
+      gc = project(s.x, s.y, alpha);
     }
-    Real f0 = 0, f1 = 0, f5 = 0;
-    double sg = 0.0, g0 = 0.0, g1 = 0.0, g5 = 0.0;
-#pragma unroll 2
-    for (int k = b + gl; k < e; k += kLanes) {
-      const V4 d = a.inc[k];
-      const double go = a.gold[k];
-      double gc = go;
-      if (mode != 0) {
-        const double2 s = ldcg(ev + k);
-        gc = project(s.x, s.y, alpha);
-      }
-      const double diff = sub(gc, go);
-      if constexpr (kF64) {
-        f0 = add(f0, mul(d.x, diff));
-        f1 = add(f1, mul(d.y, diff));
-        f5 = add(f5, mul(d.z, diff));
-        sg = add(sg, mul(d.w, gc));
-      } else {
-        const float df = (float)diff;
-        f0 = fmaf(d.x, df, f0);
-        f1 = fmaf(d.y, df, f1);
-        f5 = fmaf(d.z, df, f5);
-        sg = fma((double)d.w, gc, sg);
-      }
-      if constexpr (kTr) {
-        g0 = add(g0, mul((double)d.x, gc));
-        g1 = add(g1, mul((double)d.y, gc));
-        g5 = add(g5, mul((double)d.z, gc));
-      }
+    const double diff = sub(gc, go);
+    if constexpr (kF64) {
+      A.f0 = add(A.f0, mul(d.x, diff));
+      A.f1 = add(A.f1, mul(d.y, diff));
+      A.f5 = add(A.f5, mul(d.z, diff));
+      A.sg = add(A.sg, mul(d.w, gc));
+    } else {
+      const float df = (float)diff;
+      A.f0 = fmaf(d.x, df, A.f0);
+      A.f1 = fmaf(d.y, df, A.f1);
+      A.f5 = fmaf(d.z, df, A.f5);
+      A.sg = fma((double)d.w, gc, A.sg);
     }
+    if constexpr (kTr) {
+      A.g0 = add(A.g0, mul((double)d.x, gc));
+      A.g1 = add(A.g1, mul((double)d.y, gc));
+      A.g5 = add(A.g5, mul((double)d.z, gc));
+    }
+  };
+  auto combine = [&](CellAcc<Real>& A) {  // fixed shuffle tree over the group's lanes
 #pragma unroll
     for (int o = kLanes / 2; o > 0; o >>= 1) {
-      f0 = lane_add(f0, __shfl_xor_sync(kFull, f0, o));
-      f1 = lane_add(f1, __shfl_xor_sync(kFull, f1, o));
-      f5 = lane_add(f5, __shfl_xor_sync(kFull, f5, o));
-      sg = add(sg, __shfl_xor_sync(kFull, sg, o));
+      A.f0 = lane_add(A.f0, __shfl_xor_sync(kFull, A.f0, o));
+      A.f1 = lane_add(A.f1, __shfl_xor_sync(kFull, A.f1, o));
+      A.f5 = lane_add(A.f5, __shfl_xor_sync(kFull, A.f5, o));
+      A.sg = add(A.sg, __shfl_xor_sync(kFull, A.sg, o));
       if constexpr (kTr) {
-        g0 = add(g0, __shfl_xor_sync(kFull, g0, o));
-        g1 = add(g1, __shfl_xor_sync(kFull, g1, o));
-        g5 = add(g5, __shfl_xor_sync(kFull, g5, o));
+        A.g0 = add(A.g0, __shfl_xor_sync(kFull, A.g0, o));
+        A.g1 = add(A.g1, __shfl_xor_sync(kFull, A.g1, o));
+        A.g5 = add(A.g5, __shfl_xor_sync(kFull, A.g5, o));
       }
     }
-    if (gl != 0 || p >= a.n) continue;
+  };
+  auto finish = [&](long long p, const CellAcc<Real>& A) {
     const V4 cl = a.cell[p];
     const double uez = a.uext ? a.uext[3 * p + 2] : 0.0;
     double ux, uy, wz;
     if constexpr (kF64) {
-      ux = add(add(0.0, mul(cl.x, f0)), 0.0);
-      uy = add(add(0.0, mul(cl.x, f1)), 0.0);
-      wz = add(add(0.0, mul(cl.y, f5)), uez);  // U = U_ext + M F (HardModelGradient.cpp:21)
+      ux = add(add(0.0, mul(cl.x, A.f0)), 0.0);
+      uy = add(add(0.0, mul(cl.x, A.f1)), 0.0);
+      wz = add(add(0.0, mul(cl.y, A.f5)), uez);  // U = U_ext + M F (HardModelGradient.cpp:21)
     } else {
-      ux = cl.x * f0;
-      uy = cl.x * f1;
-      wz = (double)(cl.y * f5) + uez;
+      ux = cl.x * A.f0;
+      uy = cl.x * A.f1;
+      wz = (double)(cl.y * A.f5) + uez;
     }
-    const double im = exp(vscale(-a.lambda, sg));
+    const double im = exp(vscale(-a.lambda, A.sg));
     const double ld = vscale(dvd(1.0, a.tau), mul((double)cl.z, im));
     a.u[p] = mk4<V4>(ux, uy, wz, sub(ld, (double)cl.w));
     if constexpr (kTr) {
       const double ml = cl.x, mr = cl.y;
-      *eq = add(*eq, add(add(mul(g0, mul(ml, g0)), mul(g1, mul(ml, g1))), mul(g5, mul(mr, g5))));
+      *eq = add(*eq, add(add(mul(A.g0, mul(ml, A.g0)), mul(A.g1, mul(ml, A.g1))), mul(A.g5, mul(mr, A.g5))));
       *eg = add(*eg, mul((double)cl.z, im));
     }
     if (final) {
@@ -209,16 +211,40 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, int pa
       Up[3] = 0.0;
       Up[4] = 0.0;
       Up[5] = wz;
-      Fp[0] = f0;
-      Fp[1] = f1;
+      Fp[0] = A.f0;
+      Fp[1] = A.f1;
       Fp[2] = 0.0;
       Fp[3] = 0.0;
       Fp[4] = 0.0;
-      Fp[5] = f5;
-      a.sig[p] = sg;
+      Fp[5] = A.f5;
+      a.sig[p] = A.sg;
       a.ldot[p] = ld;
       a.imp[p] = im;
     }
+  };
+  const long long stride = U::warps() * kCellsPerWarp;
+  for (long long pw = U::warp() * kCellsPerWarp; pw < a.n; pw += 2 * stride) {
+    const long long p0 = pw + lane / kLanes, p1 = p0 + stride;
+    int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
+    if (p0 < a.n) {
+      b0 = a.inc_off[p0];
+      e0 = a.inc_off[p0 + 1];
+    }
+    if (p1 < a.n) {
+      b1 = a.inc_off[p1];
+      e1 = a.inc_off[p1 + 1];
+    }
+    CellAcc<Real> A0, A1;
+    const int n0 = e0 - b0, n1 = e1 - b1, nm = n0 > n1 ? n0 : n1;
+    for (int r = gl; r < nm; r += kLanes) {
+      if (r < n0) accumulate(A0, b0 + r);
+      if (r < n1) accumulate(A1, b1 + r);
+    }
+    combine(A0);
+    combine(A1);
+    if (gl != 0) continue;
+    if (p0 < a.n) finish(p0, A0);
+    if (p1 < a.n) finish(p1, A1);
   }
 }
 
@@ -266,11 +292,15 @@ __device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, 
   const int out = mode == 0 ? par : 1 - par;
   double2* gout = a.gg[out];
   double2* eout = a.ev[out];
+  const int S = a.per_thread;
   for (long long ch = U::unit(); ch < a.nchunks; ch += U::units()) {
     double v[4] = {0, 0, 0, 0};
     double lin = 0.0;
-    const long long c = ch * kPChunk + U::t();
-    if (c < a.m) {
+    const long long base = ch * (long long)kBlock * S + U::t();
+#pragma unroll 2
+    for (int q = 0; q < S; ++q) {
+      const long long c = base + (long long)q * kBlock;
+      if (c >= a.m) break;
       const double2 s = ldcg(gin + c);
       const double gam = mode == 0 ? s.x : project(s.x, s.y, alpha);
       const double g = planar_grad(a, c);
@@ -281,12 +311,15 @@ __device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, 
       eout[ps.y] = r;
       if (mode != 0) {
         const double dgm = sub(gam, s.x), dg = sub(g, s.y);
-        v[0] = mul(dgm, dgm);
-        v[1] = mul(dgm, dg);
-        v[2] = mul(dg, dg);
+        v[0] = add(v[0], mul(dgm, dgm));
+        v[1] = add(v[1], mul(dgm, dg));
+        v[2] = add(v[2], mul(dg, dg));
       }
-      if (mode == 0 || check) v[3] = proj_grad_abs(g, gam);
-      if constexpr (kTr) lin = mul(gam, a.phi[c]);
+      if (mode == 0 || check) {
+        const double rr = proj_grad_abs(g, gam);
+        v[3] = v[3] < rr ? rr : v[3];
+      }
+      if constexpr (kTr) lin = add(lin, mul(gam, a.phi[c]));
     }
     unit_reduce4<U>(v, sm);
     if (U::t() == 0) a.partials[ch] = make_double4(v[0], v[1], v[2], v[3]);
@@ -309,8 +342,10 @@ __device__ __forceinline__ void trace_cells(double* smt, double eq, double eg, d
   }
 }
 
+// Four blocks per SM fit the register file (64 registers a thread), which
+// the chunk sizing (kChunkTarget) assumes.
 template <class Real, int kTr>
-__global__ void __launch_bounds__(kBlock) k_bbpgd_planar(PArgs<Real> a) {
+__global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real> a) {
   __shared__ double sm[4 * (kBlock / 32)];
   __shared__ double smt[kTr ? 4 * kBlock : 1];
   const int TR = kTr ? a.trace : 0;
@@ -535,7 +570,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
       (e = B::inc(ctx).reserve(ne + 1, 0, s)) || (e = B::cell(ctx).reserve(nn, 0, s)) ||
       (e = B::u(ctx).reserve(nn, 0, s)))
     return e;
-  const long long nchunks = (long long)((m + kPChunk - 1) / kPChunk);
+  const long long nchunks = chunk_count((long long)m);
   if ((e = ctx->partials.reserve(4 * (nchunks + 1), 0, s))) return e;
   ConsView cv = ctx->cons.view();
   if (m) {
@@ -583,6 +618,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   a.max_it = ctx->params.max_bbpgd_iterations;
   a.partials = reinterpret_cast<double4*>(ctx->partials.p);
   a.nchunks = nchunks;
+  a.per_thread = chunk_per_thread((long long)m);
   a.sc = ctx->scal.p;
   a.st_err = ctx->status;
   a.trace = tr.trace;
@@ -617,7 +653,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
 
 }  // namespace
 
-long long planar_chunks(size_t m) { return (long long)((m + kPChunk - 1) / kPChunk); }
+long long planar_chunks(size_t m) { return chunk_count((long long)m); }
 
 cudaError_t planar_bbpgd(pcc_ctx* ctx, double dt, bool mixed, const PlanarTrace& tr, int* kind) {
   return mixed ? launch<float>(ctx, dt, tr, kind) : launch<double>(ctx, dt, tr, kind);

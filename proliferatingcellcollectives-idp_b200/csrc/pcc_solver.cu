@@ -10,8 +10,8 @@
 //     in a fixed shuffle tree; no atomics), U = M F, growth rate and its change;
 //   constraint pass, one thread per constraint: phi_next = Phi + dt D U -
 //     dt L dldot, the projected-gradient residual and the three
-//     Barzilai-Borwein dot products, reduced per fixed chunk of kPChunk
-//     constraints.
+//     Barzilai-Borwein dot products, reduced per fixed chunk of constraints
+//     (chunk_per_thread).
 // The projection gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0) is recomputed
 // where it is needed (both passes), so no extra pass stores it.  The last block
 // to reach a barrier reduces the chunk partials in a fixed order and publishes
@@ -207,11 +207,14 @@ __device__ __forceinline__ void constraint_pass(const SolverArgs& a, int mode, c
                                                 double* gam_out, double* g_out, double alpha, bool check, double* sm,
                                                 double* smt) {
   double4* partials = reinterpret_cast<double4*>(a.partials);
+  const int S = chunk_per_thread(a.m);
   for (long long ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
     double v[4] = {0, 0, 0, 0};  // sum dgam^2, sum dgam*dg, sum dg^2, max residual
     double lin = 0.0;
-    const long long c = ch * kPChunk + threadIdx.x;
-    if (c < a.m) {
+    const long long base = ch * (long long)kBlock * S + threadIdx.x;
+    for (int q = 0; q < S; ++q) {
+      const long long c = base + (long long)q * kBlock;
+      if (c >= a.m) break;
       const double gpc = mode == 0 ? a.gamma[c] : ldcg(gp + c), ggc = mode == 0 ? 0.0 : ldcg(gg + c);
       const double gam = mode == 0 ? gpc : project(gpc, ggc, alpha);
       const double g = constraint_grad(a, c);
@@ -219,12 +222,15 @@ __device__ __forceinline__ void constraint_pass(const SolverArgs& a, int mode, c
       g_out[c] = g;
       if (mode != 0) {
         const double dgm = sub(gam, gpc), dg = sub(g, ggc);
-        v[0] = mul(dgm, dgm);
-        v[1] = mul(dgm, dg);
-        v[2] = mul(dg, dg);
+        v[0] = add(v[0], mul(dgm, dgm));
+        v[1] = add(v[1], mul(dgm, dg));
+        v[2] = add(v[2], mul(dg, dg));
       }
-      if (mode == 0 || check) v[3] = proj_grad_abs(g, gam);
-      if constexpr (kTr) lin = mul(gam, a.phi[c]);
+      if (mode == 0 || check) {
+        const double rr = proj_grad_abs(g, gam);
+        v[3] = v[3] < rr ? rr : v[3];
+      }
+      if constexpr (kTr) lin = add(lin, mul(gam, a.phi[c]));
     }
     unit_reduce4<GridUnits>(v, sm);
     if (threadIdx.x == 0) partials[ch] = make_double4(v[0], v[1], v[2], v[3]);
@@ -568,7 +574,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     return e;
   if ((e = ctx->scal.reserve(1, 0, s))) return e;
   cudaMemsetAsync(ctx->scal.p, 0, sizeof(SolverScalars), s);
-  const long long nchunks = planar_chunks(m);  // kPChunk constraints per chunk, as the planar kernels
+  const long long nchunks = planar_chunks(m);  // the planar kernels' chunks
   const bool tracing = ctx->trace_active;
   long long trace_cap = 0;
   if (tracing) {
