@@ -57,84 +57,89 @@ __device__ __forceinline__ double vscale(double a, double x) {
   return mul(a, x);
 }
 
-__device__ __forceinline__ bool barrier(SolverScalars* sc, unsigned nblocks, DevStatus* st) {
-  if (nblocks == 1) {  // one block: a block barrier orders its global writes
+// Grid barrier of a cooperative launch.  Every block adds one to a
+// monotonic arrival counter; the k-th barrier of the launch is passed once the
+// counter reaches k * blocks, so the last arrival's own atomic releases it
+// (no reset, no second write).  sync_reduce additionally lets the last
+// arriving block run `reduce` (all its threads) and then publish the
+// barrier's ordinal in `released`, which the other blocks wait for.  Waits
+// spin at most kSpinLimit times, then raise kDevErrTimeout and report false.
+struct GridBarrier {
+  SolverScalars* sc;
+  DevStatus* st;
+  unsigned nblocks;
+  unsigned long long k = 0;  // barriers passed so far (the same in every block)
+
+  __device__ bool sync() {
+    ++k;
+    if (nblocks == 1) {  // one block: a block barrier orders its global writes
+      __syncthreads();
+      return true;
+    }
+    __shared__ int s_ok;
     __syncthreads();
-    return true;
-  }
-  __shared__ unsigned s_gen;
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_ok = 1;
-    s_gen = *(volatile unsigned*)&sc->gen;
-    __threadfence();
-    unsigned t = atomicAdd(&sc->count, 1u);
-    if (t == nblocks - 1) {
-      sc->count = 0;
+    if (threadIdx.x == 0) {
+      s_ok = 1;
+      const unsigned long long target = k * nblocks;
       __threadfence();
-      atomicAdd(&sc->gen, 1u);
-    } else {
+      if (atomicAdd(&sc->arrive, 1ULL) + 1 != target) {
+        long long spins = 0;
+        while (*(volatile unsigned long long*)&sc->arrive < target) {
+          __nanosleep(32);
+          if (++spins > kSpinLimit) {
+            raise_error(st, kDevErrTimeout, 20);
+            s_ok = 0;
+            break;
+          }
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    return s_ok;
+  }
+
+  template <typename R>
+  __device__ bool sync_reduce(R reduce) {
+    ++k;
+    if (nblocks == 1) {
+      __syncthreads();
+      reduce();
+      __syncthreads();
+      return true;
+    }
+    __shared__ int s_last, s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_ok = 1;
+      __threadfence();
+      s_last = atomicAdd(&sc->arrive, 1ULL) + 1 == k * nblocks;
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      reduce();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        *(volatile unsigned long long*)&sc->released = k;
+      }
+    } else if (threadIdx.x == 0) {
       long long spins = 0;
-      while (*(volatile unsigned*)&sc->gen == s_gen) {
-        __nanosleep(40);
+      while (*(volatile unsigned long long*)&sc->released < k) {
+        __nanosleep(32);
         if (++spins > kSpinLimit) {
-          raise_error(st, kDevErrTimeout, 20);
+          raise_error(st, kDevErrTimeout, 21);
           s_ok = 0;
           break;
         }
       }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return s_ok;
-}
-
-// Barrier whose last arriving block first runs `reduce` (all its threads).
-template <typename R>
-__device__ __forceinline__ bool barrier_reduce(SolverScalars* sc, unsigned nblocks, DevStatus* st, R reduce) {
-  if (nblocks == 1) {
-    __syncthreads();
-    reduce();
-    __syncthreads();
-    return true;
-  }
-  __shared__ unsigned s_gen;
-  __shared__ int s_last, s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_ok = 1;
-    s_gen = *(volatile unsigned*)&sc->gen;
-    __threadfence();
-    unsigned t = atomicAdd(&sc->count, 1u);
-    s_last = (t == nblocks - 1);
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    reduce();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      sc->count = 0;
       __threadfence();
-      atomicAdd(&sc->gen, 1u);
     }
-  } else if (threadIdx.x == 0) {
-    long long spins = 0;
-    while (*(volatile unsigned*)&sc->gen == s_gen) {
-      __nanosleep(40);
-      if (++spins > kSpinLimit) {
-        raise_error(st, kDevErrTimeout, 21);
-        s_ok = 0;
-        break;
-      }
-    }
-    __threadfence();
+    __syncthreads();
+    return s_ok;
   }
-  __syncthreads();
-  return s_ok;
-}
+};
 
 __device__ __forceinline__ double proj_grad_abs(double g, double gam) {
   double v = gam > 0 ? g : (g < 0.0 ? g : 0.0);

@@ -67,15 +67,19 @@ struct ConsBufs {
 };
 
 // Grid barrier + reduction scratch of the persistent solver kernel.
+// The arrival counter sits on a cache line of its own: every block adds to
+// it at every grid barrier, while the release word and the scalars that the
+// blocks read after a release share the next line.
 struct SolverScalars {
-  unsigned count;       // arrivals at the current barrier
-  unsigned gen;         // barrier generation
-  int converged;        // 1 once the residual test passed
+  unsigned long long arrive;     // block arrivals at grid barriers, monotonic within a launch
+  unsigned long long pad0[15];
+  unsigned long long released;   // ordinal of the last barrier whose reduction was published
+  int converged;                 // 1 once the residual test passed
   int pad;
-  long long iterations; // BBPGD iteration count at exit
-  double alpha;         // current step size
-  double residual;      // last evaluated residual
-  double res0;          // initial residual
+  long long iterations;          // BBPGD iteration count at exit
+  double alpha;                  // current step size
+  double residual;               // last evaluated residual
+  double res0;                   // initial residual
 };
 
 }  // namespace pcc

@@ -130,7 +130,8 @@ struct CellAcc {
 
 // Cell pass.  mode 0: gamma = gamma_0 (the initial gradient); mode 1: gamma_k
 // projected from the (gamma, g) of buffer `par` with step alpha.  A lane group
-// takes two cells per round (p and p + stride) so the loads of both are in
+// takes one cell per round and loads the next cell's incidence range and
+// record while it walks the current cell's entries, so the two loads are in
 // flight together; each cell's sums do not depend on which group takes it.
 template <class Real, class U, int kTr>
 __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, int par, double alpha, bool final,
@@ -181,9 +182,7 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, int pa
       }
     }
   };
-  auto finish = [&](long long p, const CellAcc<Real>& A) {
-    const V4 cl = a.cell[p];
-    const double uez = a.uext ? a.uext[3 * p + 2] : 0.0;
+  auto finish = [&](long long p, const CellAcc<Real>& A, const V4& cl, double uez) {
     double ux, uy, wz;
     if constexpr (kF64) {
       ux = add(add(0.0, mul(cl.x, A.f0)), 0.0);
@@ -223,28 +222,36 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, int pa
     }
   };
   const long long stride = U::warps() * kCellsPerWarp;
-  for (long long pw = U::warp() * kCellsPerWarp; pw < a.n; pw += 2 * stride) {
-    const long long p0 = pw + lane / kLanes, p1 = p0 + stride;
-    int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
-    if (p0 < a.n) {
-      b0 = a.inc_off[p0];
-      e0 = a.inc_off[p0 + 1];
+  long long p = U::warp() * kCellsPerWarp + lane / kLanes;
+  int b = 0, e = 0;
+  V4 cl{};
+  double uez = 0.0;
+  if (p < a.n) {
+    b = a.inc_off[p];
+    e = a.inc_off[p + 1];
+    cl = a.cell[p];
+    if (a.uext) uez = a.uext[3 * p + 2];
+  }
+  for (long long pw = U::warp() * kCellsPerWarp; pw < a.n; pw += stride) {
+    const long long pn = p + stride;
+    int bn = 0, en = 0;
+    V4 cln{};
+    double uezn = 0.0;
+    if (pn < a.n) {
+      bn = a.inc_off[pn];
+      en = a.inc_off[pn + 1];
+      cln = a.cell[pn];
+      if (a.uext) uezn = a.uext[3 * pn + 2];
     }
-    if (p1 < a.n) {
-      b1 = a.inc_off[p1];
-      e1 = a.inc_off[p1 + 1];
-    }
-    CellAcc<Real> A0, A1;
-    const int n0 = e0 - b0, n1 = e1 - b1, nm = n0 > n1 ? n0 : n1;
-    for (int r = gl; r < nm; r += kLanes) {
-      if (r < n0) accumulate(A0, b0 + r);
-      if (r < n1) accumulate(A1, b1 + r);
-    }
-    combine(A0);
-    combine(A1);
-    if (gl != 0) continue;
-    if (p0 < a.n) finish(p0, A0);
-    if (p1 < a.n) finish(p1, A1);
+    CellAcc<Real> A;
+    for (int k = b + gl; k < e; k += kLanes) accumulate(A, k);
+    combine(A);
+    if (gl == 0 && p < a.n) finish(p, A, cl, uez);
+    p = pn;
+    b = bn;
+    e = en;
+    cl = cln;
+    uez = uezn;
   }
 }
 
@@ -351,6 +358,7 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
   const int TR = kTr ? a.trace : 0;
   const unsigned nb = gridDim.x;
   SolverScalars* sc = a.sc;
+  GridBarrier bar{sc, a.st_err, nb};
 
   // gradient at gamma_0 and the initial residual (BBPGD.cpp:40-44)
   {
@@ -358,7 +366,7 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
     cell_pass<Real, GridUnits, kTr>(a, 0, 0, 0.0, false, &eq, &eg);
     if (TR) trace_cells(smt, eq, eg, a.tr_part);
   }
-  if (!barrier(sc, nb, a.st_err)) return;
+  if (!bar.sync()) return;
   constraint_pass<Real, GridUnits, kTr>(a, 0, 0, 0.0, true, sm, smt);
   auto reduce_init = [&]() {
     double v[4];
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
       trace_record(smt, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
                    a.trace_cap);
   };
-  if (!barrier_reduce(sc, nb, a.st_err, reduce_init)) return;
+  if (!bar.sync_reduce(reduce_init)) return;
 
   int p = 0;  // buffer holding gamma_{k-1}, g_{k-1}
   long long it = 1;
@@ -386,7 +394,7 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
       cell_pass<Real, GridUnits, kTr>(a, 1, p, alpha, check, &eq, &eg);
       if (TR) trace_cells(smt, eq, eg, a.tr_part);
     }
-    if (!barrier(sc, nb, a.st_err)) return;
+    if (!bar.sync()) return;
     constraint_pass<Real, GridUnits, kTr>(a, 1, p, alpha, check, sm, smt);
     auto reduce_iter = [&]() {
       double v[4];
@@ -406,7 +414,7 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
         sc->iterations = it;
       }
     };
-    if (!barrier_reduce(sc, nb, a.st_err, reduce_iter)) return;
+    if (!bar.sync_reduce(reduce_iter)) return;
     if (*(volatile int*)&sc->converged) break;
     p = 1 - p;
     ++it;

@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
   const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x;
   const long long stride = (long long)nb * kBlock;
   SolverScalars* sc = a.sc;
+  GridBarrier bar{sc, a.st, nb};
   const double4* partials = reinterpret_cast<const double4*>(a.partials);
 
   // ---- gradient at gamma_0 and the initial residual (BBPGD.cpp:40-44)
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
     cell_pass<kTr>(a, 0, nullptr, nullptr, 0.0, false, &eq, &eg);
     if (TR) trace_cells(smt, eq, eg, a.tr_part);
   }
-  if (!barrier(sc, nb, a.st)) return;
+  if (!bar.sync()) return;
   constraint_pass<kTr>(a, 0, nullptr, nullptr, a.gam[0], a.g[0], 0.0, true, sm, smt);
   auto reduce_init = [&]() {
     double v[4];
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
       trace_record(smt, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
                    a.trace_cap);
   };
-  if (!barrier_reduce(sc, nb, a.st, reduce_init)) return;
+  if (!bar.sync_reduce(reduce_init)) return;
 
   int p = 0;  // buffer of gamma_{k-1}, g_{k-1}
   long long it = 1;
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
       cell_pass<kTr>(a, 1, a.gam[p], a.g[p], alpha, check, &eq, &eg);
       if (TR) trace_cells(smt, eq, eg, a.tr_part);
     }
-    if (!barrier(sc, nb, a.st)) return;
+    if (!bar.sync()) return;
     constraint_pass<kTr>(a, 1, a.gam[p], a.g[p], a.gam[1 - p], a.g[1 - p], alpha, check, sm, smt);
     auto reduce_iter = [&]() {
       double v[4];
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(kBlock) k_bbpgd(SolverArgs a) {
         sc->iterations = it;
       }
     };
-    if (!barrier_reduce(sc, nb, a.st, reduce_iter)) return;
+    if (!bar.sync_reduce(reduce_iter)) return;
     if (*(volatile int*)&sc->converged) break;
     p = 1 - p;
     ++it;
