@@ -64,6 +64,29 @@ __device__ __forceinline__ double vscale(double a, double x) {
 // arriving block run `reduce` (all its threads) and then publish the
 // barrier's ordinal in `released`, which the other blocks wait for.  Waits
 // spin at most kSpinLimit times, then raise kDevErrTimeout and report false.
+__device__ __forceinline__ unsigned long long atom_add_release(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long atom_add_acq_rel(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// The block's writes before a barrier are ordered before thread 0's release
+// by the preceding bar.sync (the release is cumulative); thread 0's acquire,
+// followed by bar.sync, orders the other blocks' writes before every thread's
+// later reads.
 struct GridBarrier {
   SolverScalars* sc;
   DevStatus* st;
@@ -81,10 +104,9 @@ struct GridBarrier {
     if (threadIdx.x == 0) {
       s_ok = 1;
       const unsigned long long target = k * nblocks;
-      __threadfence();
-      if (atomicAdd(&sc->arrive, 1ULL) + 1 != target) {
+      if (atom_add_acq_rel(&sc->arrive, 1ULL) + 1 != target) {
         long long spins = 0;
-        while (*(volatile unsigned long long*)&sc->arrive < target) {
+        while (ld_acquire(&sc->arrive) < target) {
           __nanosleep(32);
           if (++spins > kSpinLimit) {
             raise_error(st, kDevErrTimeout, 20);
@@ -93,7 +115,6 @@ struct GridBarrier {
           }
         }
       }
-      __threadfence();
     }
     __syncthreads();
     return s_ok;
@@ -112,21 +133,16 @@ struct GridBarrier {
     __syncthreads();
     if (threadIdx.x == 0) {
       s_ok = 1;
-      __threadfence();
-      s_last = atomicAdd(&sc->arrive, 1ULL) + 1 == k * nblocks;
+      s_last = atom_add_acq_rel(&sc->arrive, 1ULL) + 1 == k * nblocks;
     }
     __syncthreads();
     if (s_last) {
-      __threadfence();
       reduce();
       __syncthreads();
-      if (threadIdx.x == 0) {
-        __threadfence();
-        *(volatile unsigned long long*)&sc->released = k;
-      }
+      if (threadIdx.x == 0) st_release(&sc->released, k);
     } else if (threadIdx.x == 0) {
       long long spins = 0;
-      while (*(volatile unsigned long long*)&sc->released < k) {
+      while (ld_acquire(&sc->released) < k) {
         __nanosleep(32);
         if (++spins > kSpinLimit) {
           raise_error(st, kDevErrTimeout, 21);
@@ -134,7 +150,6 @@ struct GridBarrier {
           break;
         }
       }
-      __threadfence();
     }
     __syncthreads();
     return s_ok;

@@ -124,8 +124,8 @@ struct pcc_ctx {
   pcc::DevBuf<double> fel;  // soft: Hertz force magnitude per contact
   // packed operands of the planar solver
   pcc::DevBuf<int2> p_ij, p_pos;
-  pcc::DevBuf<double2> p_n, p_t, p_s, p_gg0, p_gg1, p_ev0, p_ev1;
-  pcc::DevBuf<double> p_gold;
+  pcc::DevBuf<double2> p_n, p_t, p_s, p_gg, p_ev;
+  pcc::DevBuf<double> p_gold, p_phin;
   pcc::DevBuf<double4> p_inc, p_cell, p_u;
   // ... their FP32 forms (mixed precision)
   pcc::DevBuf<float2> pf_n, pf_t, pf_s;

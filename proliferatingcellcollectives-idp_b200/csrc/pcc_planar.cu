@@ -18,11 +18,17 @@
 //     by a fixed shuffle tree, and the first lane forms U = M F, the growth
 //     rate and its change;
 //   constraint pass: a few constraints per thread in fixed chunks
-//     (chunk_per_thread), phi_next = Phi + dt D U - dt L dldot, the new (gamma_k, g_k) written to
-//     the constraint and pushed to its two incidence entries (so the next
-//     cell pass reads them in order instead of gathering), and the three
-//     Barzilai-Borwein dot products and the residual reduced per chunk by a
-//     fixed shuffle tree.
+//     (chunk_per_thread), phi_next = Phi + dt D U - dt L dldot, the new
+//     (gamma_k, g_k) written over the constraint's previous pair and pushed
+//     over its two incidence entries (so the next cell pass reads them in
+//     order instead of gathering), and the three Barzilai-Borwein dot
+//     products and the residual reduced per chunk by a fixed shuffle tree.
+// The (gamma, g) pairs are updated in place: the cell pass reads the entry
+// copies before the first barrier and the constraint pass rewrites them
+// after it, and each constraint's pair is read and rewritten by the same
+// thread.  On residual iterations (the only ones that can end the solve) the
+// constraint pass also stores gamma_{k-1}, the iterate the reference returns,
+// and phi_next, so nothing has to be kept from the previous iteration.
 // The last block to reach the second barrier reduces the chunk partials in a
 // fixed order and publishes the step size and the convergence decision.  The
 // work of a chunk and of a cell never depends on which block does it, so the
@@ -93,12 +99,13 @@ struct PArgs {
   const int2* pos;         // incidence entries of side i and side j
   double* phi;             // Phi on entry, phi_next of the returned iterate on exit
   double* gamma;           // gamma_0 on entry, gamma_{k-1} on exit
-  double2* gg[2];          // (gamma, g), ping-pong per iteration
+  double* phin;            // phi_next of the last residual iteration
+  double2* gg;             // (gamma, g) of the last iteration
   // per incidence entry
   const int* inc_off;
   const V4* inc;           // (D_x, D_y, D_t, s) of that side
   const double* gold;      // gamma_old of the entry's constraint
-  double2* ev[2];          // the entry's constraint's (gamma, g), ping-pong like gg
+  double2* ev;             // the entry's constraint's (gamma, g), a copy of gg
   // per cell
   const V4* cell;          // (M_lin, M_rot, len, ldot_prev)
   V4* u;                   // (u_x, u_y, w_z, dldot)
@@ -129,18 +136,18 @@ struct CellAcc {
 };
 
 // Cell pass.  mode 0: gamma = gamma_0 (the initial gradient); mode 1: gamma_k
-// projected from the (gamma, g) of buffer `par` with step alpha.  A lane group
+// projected from the entries' (gamma, g) with step alpha.  A lane group
 // takes one cell per round and loads the next cell's incidence range and
 // record while it walks the current cell's entries, so the two loads are in
 // flight together; each cell's sums do not depend on which group takes it.
 template <class Real, class U, int kTr>
-__device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, int par, double alpha, bool final,
-                                          double* eq, double* eg) {
+__device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double alpha, bool final, double* eq,
+                                          double* eg) {
   using V4 = typename PT<Real>::V4;
   constexpr bool kF64 = sizeof(Real) == 8;
   const int lane = threadIdx.x & 31, gl = lane % kLanes;
   constexpr long long kCellsPerWarp = 32 / kLanes;
-  const double2* ev = a.ev[par];
+  const double2* ev = a.ev;
   auto accumulate = [&](CellAcc<Real>& A, int k) {
     const V4 d = a.inc[k];
     const double go = a.gold[k];
@@ -289,16 +296,14 @@ __device__ __forceinline__ double planar_grad(const PArgs<Real>& a, long long c)
   }
 }
 
-// Constraint pass: new (gamma, g) into buffer `out` and the incidence
-// entries, chunk partials.  mode 0 evaluates g at gamma_0 (in place, residual
+// Constraint pass: new (gamma, g) over the constraint's pair and its two
+// incidence entries, chunk partials.  mode 0 evaluates g at gamma_0 (residual
 // only).
 template <class Real, class U, int kTr>
-__device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, int par, double alpha, bool check,
-                                                double* sm, double* smt) {
-  const double2* gin = a.gg[par];
-  const int out = mode == 0 ? par : 1 - par;
-  double2* gout = a.gg[out];
-  double2* eout = a.ev[out];
+__device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, double alpha, bool check, double* sm,
+                                                double* smt) {
+  double2* gg = a.gg;
+  double2* eout = a.ev;
   const int S = a.per_thread;
   for (long long ch = U::unit(); ch < a.nchunks; ch += U::units()) {
     double v[4] = {0, 0, 0, 0};
@@ -308,11 +313,15 @@ __device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, 
     for (int q = 0; q < S; ++q) {
       const long long c = base + (long long)q * kBlock;
       if (c >= a.m) break;
-      const double2 s = ldcg(gin + c);
+      const double2 s = gg[c];
       const double gam = mode == 0 ? s.x : project(s.x, s.y, alpha);
       const double g = planar_grad(a, c);
       const double2 r = make_double2(gam, g);
-      gout[c] = r;
+      gg[c] = r;
+      if (mode != 0 && check) {  // what the solve returns if it ends here (Hard.cpp:170, BBPGD.cpp:124)
+        a.gamma[c] = s.x;
+        a.phin[c] = g;
+      }
       const int2 ps = a.pos[c];
       eout[ps.x] = r;
       eout[ps.y] = r;
@@ -363,11 +372,11 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
   // gradient at gamma_0 and the initial residual (BBPGD.cpp:40-44)
   {
     double eq = 0.0, eg = 0.0;
-    cell_pass<Real, GridUnits, kTr>(a, 0, 0, 0.0, false, &eq, &eg);
+    cell_pass<Real, GridUnits, kTr>(a, 0, 0.0, false, &eq, &eg);
     if (TR) trace_cells(smt, eq, eg, a.tr_part);
   }
   if (!bar.sync()) return;
-  constraint_pass<Real, GridUnits, kTr>(a, 0, 0, 0.0, true, sm, smt);
+  constraint_pass<Real, GridUnits, kTr>(a, 0, 0.0, true, sm, smt);
   auto reduce_init = [&]() {
     double v[4];
     reduce_partials<GridUnits>(a.partials, a.nchunks, v, sm);
@@ -383,7 +392,6 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
   };
   if (!bar.sync_reduce(reduce_init)) return;
 
-  int p = 0;  // buffer holding gamma_{k-1}, g_{k-1}
   long long it = 1;
   while (it < a.max_it) {
     const double alpha = *(volatile double*)&sc->alpha;
@@ -391,11 +399,11 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
     const bool check = (it % 10) == 0 || TR;
     {
       double eq = 0.0, eg = 0.0;
-      cell_pass<Real, GridUnits, kTr>(a, 1, p, alpha, check, &eq, &eg);
+      cell_pass<Real, GridUnits, kTr>(a, 1, alpha, check, &eq, &eg);
       if (TR) trace_cells(smt, eq, eg, a.tr_part);
     }
     if (!bar.sync()) return;
-    constraint_pass<Real, GridUnits, kTr>(a, 1, p, alpha, check, sm, smt);
+    constraint_pass<Real, GridUnits, kTr>(a, 1, alpha, check, sm, smt);
     auto reduce_iter = [&]() {
       double v[4];
       reduce_partials<GridUnits>(a.partials, a.nchunks, v, sm);
@@ -416,17 +424,14 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real
     };
     if (!bar.sync_reduce(reduce_iter)) return;
     if (*(volatile int*)&sc->converged) break;
-    p = 1 - p;
     ++it;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) sc->iterations = it;
   if (!*(volatile int*)&sc->converged) return;
-  // returned result (Hard.cpp:170 with BBPGD.cpp:124): gamma_{k-1}, phi(gamma_k)
+  // returned result (Hard.cpp:170 with BBPGD.cpp:124): gamma_{k-1} (stored by
+  // the last constraint pass), phi of gamma_k
   const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x, stride = (long long)nb * kBlock;
-  for (long long c = tid; c < a.m; c += stride) {
-    a.gamma[c] = ldcg(a.gg[p] + c).x;
-    a.phi[c] = ldcg(a.gg[1 - p] + c).y;
-  }
+  for (long long c = tid; c < a.m; c += stride) a.phi[c] = ldcg(a.phin + c);
 }
 
 // One-CTA form for colonies of up to kCtaCells cells and kCtaConstraints
@@ -441,9 +446,9 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_bbpgd_planar_cta(PArgs<Real>
   const unsigned unit = CtaUnits::unit();
   SolverScalars* sc = a.sc;
 
-  cell_pass<Real, CtaUnits, 0>(a, 0, 0, 0.0, false, nullptr, nullptr);
+  cell_pass<Real, CtaUnits, 0>(a, 0, 0.0, false, nullptr, nullptr);
   __syncthreads();
-  constraint_pass<Real, CtaUnits, 0>(a, 0, 0, 0.0, true, sm[unit], nullptr);
+  constraint_pass<Real, CtaUnits, 0>(a, 0, 0.0, true, sm[unit], nullptr);
   __syncthreads();
   if (unit == 0) {
     double v[4];
@@ -457,14 +462,13 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_bbpgd_planar_cta(PArgs<Real>
   }
   __syncthreads();
 
-  int p = 0;
   long long it = 1;
   while (it < a.max_it) {
     const double alpha = s_alpha;
     const bool check = (it % 10) == 0;
-    cell_pass<Real, CtaUnits, 0>(a, 1, p, alpha, check, nullptr, nullptr);
+    cell_pass<Real, CtaUnits, 0>(a, 1, alpha, check, nullptr, nullptr);
     __syncthreads();
-    constraint_pass<Real, CtaUnits, 0>(a, 1, p, alpha, check, sm[unit], nullptr);
+    constraint_pass<Real, CtaUnits, 0>(a, 1, alpha, check, sm[unit], nullptr);
     __syncthreads();
     if (unit == 0) {
       double v[4];
@@ -482,7 +486,6 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_bbpgd_planar_cta(PArgs<Real>
     }
     __syncthreads();
     if (s_conv) break;
-    p = 1 - p;
     ++it;
   }
   if (threadIdx.x == 0) {
@@ -491,10 +494,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_bbpgd_planar_cta(PArgs<Real>
     sc->alpha = s_alpha;
   }
   if (!s_conv) return;
-  for (long long c = threadIdx.x; c < a.m; c += kCtaThreads) {
-    a.gamma[c] = ldcg(a.gg[p] + c).x;
-    a.phi[c] = ldcg(a.gg[1 - p] + c).y;
-  }
+  for (long long c = threadIdx.x; c < a.m; c += kCtaThreads) a.phi[c] = a.phin[c];
 }
 
 // ---------------------------------------------------------------- packing
@@ -570,9 +570,9 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   const size_t n = ctx->n, m = ctx->ncons, ne = 2 * m;
   const size_t mm = m + 1, nn = n + 1;
   cudaError_t e;
-  if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_pos.reserve(mm, 0, s)) || (e = ctx->p_gg0.reserve(mm, 0, s)) ||
-      (e = ctx->p_gg1.reserve(mm, 0, s)) || (e = ctx->p_gold.reserve(ne + 1, 0, s)) ||
-      (e = ctx->p_ev0.reserve(ne + 1, 0, s)) || (e = ctx->p_ev1.reserve(ne + 1, 0, s)))
+  if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_pos.reserve(mm, 0, s)) || (e = ctx->p_gg.reserve(mm, 0, s)) ||
+      (e = ctx->p_phin.reserve(mm, 0, s)) || (e = ctx->p_gold.reserve(ne + 1, 0, s)) ||
+      (e = ctx->p_ev.reserve(ne + 1, 0, s)))
     return e;
   if ((e = B::nn(ctx).reserve(mm, 0, s)) || (e = B::tt(ctx).reserve(mm, 0, s)) || (e = B::ss(ctx).reserve(mm, 0, s)) ||
       (e = B::inc(ctx).reserve(ne + 1, 0, s)) || (e = B::cell(ctx).reserve(nn, 0, s)) ||
@@ -583,7 +583,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   ConsView cv = ctx->cons.view();
   if (m) {
     k_pack_planar_cons<Real><<<grid_for((long long)m), kBlock, 0, s>>>(cv, (long long)m, ctx->p_ij.p, B::nn(ctx).p,
-                                                                       B::tt(ctx).p, B::ss(ctx).p, ctx->p_gg0.p);
+                                                                       B::tt(ctx).p, B::ss(ctx).p, ctx->p_gg.p);
     k_pack_planar_inc<Real><<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne,
                                                                        B::inc(ctx).p, ctx->p_gold.p,
                                                                        reinterpret_cast<int*>(ctx->p_pos.p));
@@ -604,13 +604,12 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   a.pos = ctx->p_pos.p;
   a.phi = cv.sd;
   a.gamma = cv.gamma;
-  a.gg[0] = ctx->p_gg0.p;
-  a.gg[1] = ctx->p_gg1.p;
+  a.phin = ctx->p_phin.p;
+  a.gg = ctx->p_gg.p;
   a.inc_off = ctx->inc_off.p;
   a.inc = B::inc(ctx).p;
   a.gold = ctx->p_gold.p;
-  a.ev[0] = ctx->p_ev0.p;
-  a.ev[1] = ctx->p_ev1.p;
+  a.ev = ctx->p_ev.p;
   a.cell = B::cell(ctx).p;
   a.u = B::u(ctx).p;
   a.uext = ctx->uext_active ? ctx->uext.p : nullptr;
