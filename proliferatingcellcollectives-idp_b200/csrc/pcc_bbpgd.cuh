@@ -23,7 +23,7 @@ constexpr int kTraceWidth = 8;  // it, residual, step size, linear, quadratic, g
 // most kChunkTarget chunks, one round of a grid of four 256-thread blocks on
 // each of 148 SMs, so every block reduces one chunk per iteration with S
 // independent constraints in flight per thread.  Nothing depends on the grid.
-constexpr int kLanes = 4;
+constexpr int kLanes = 2;
 constexpr long long kChunkTarget = 592;
 constexpr int kMaxPerThread = 8;
 __host__ __device__ inline int chunk_per_thread(long long m) {
