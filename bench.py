@@ -449,6 +449,8 @@ def run_grow(args):
     cells = 0.0
     radius = 0.0
     marks = []
+    from collections import deque
+    tail = deque(maxlen=50)  # solver statistics of the last steps, kept with a saved snapshot
     e0.record(stream)
     st = {}
     while radius < args.radius and time.time() - t0 < args.grow_seconds:
@@ -464,12 +466,15 @@ def run_grow(args):
             tlast = time.time()
             print(json.dumps({"step": steps, "radius": radius, "cells": st["n_cells"], "dt": st["dt_used"],
                               "bbpgd": st["bbpgd_iterations"], "wall_s": tlast - t0}), file=sys.stderr, flush=True)
+        tail.append(st)
     e1.record(stream)
     e1.synchronize()
     wall = time.time() - t0
     dev_ms = e0.elapsed_time(e1)
     prof = col.profile()
     final = col.get_cells()
+    if args.save:
+        save_snapshot(args.save, final, col.dt, steps, st, tail, args.job_seed)
     print(json.dumps({
         "grow": True, "precision": args.precision, "radius_target": args.radius, "radius": radius,
         "reached": radius >= args.radius, "steps": steps, "cells": int(st.get("n_cells", 1)),
@@ -478,6 +483,36 @@ def run_grow(args):
         "stage_ms": {"bbpgd": prof["bbpgd_ms"], "detect": prof["detect_ms"], "solve": prof["solve_ms"]},
         "packing_fraction": packing_fraction(final), "sim_time": st.get("sim_time"), "marks": marks,
     }), flush=True)
+
+
+def save_snapshot(path: str, cells: dict, dt: float, steps: int, last: dict, tail: list, seed: int):
+    """A grown colony as the benchmark's starting state: centres, orientation
+    angle and length as float32 (the start of a step tolerates the rounding:
+    it moves cells by < 3e-5, far below the solver tolerance), birth length and
+    diameter as float32, age as int32, with the run that made it."""
+    th = 2.0 * np.arctan2(np.asarray(cells["q3"]), np.asarray(cells["q0"]))
+    np.savez_compressed(path, x=np.asarray(cells["x"], np.float32), y=np.asarray(cells["y"], np.float32),
+                        theta=th.astype(np.float32), length=np.asarray(cells["length"], np.float32),
+                        l0=np.asarray(cells["l0"], np.float32), diameter=np.asarray(cells["diameter"], np.float32),
+                        age=np.asarray(cells["age"], np.int32), dt=np.float64(dt), steps=np.int64(steps),
+                        seed=np.int64(seed), radius=np.float64(last.get("colony_radius", 0.0)),
+                        tail_bbpgd=np.array([t["bbpgd_iterations"] for t in tail], np.int64),
+                        tail_relcp=np.array([t["relcp_iterations"] for t in tail], np.int64),
+                        tail_cells=np.array([t["n_cells"] for t in tail], np.int64))
+
+
+def load_snapshot(path: str) -> tuple[dict, float, dict]:
+    """Cells of a saved grown colony (float64, planar: z = 0, rotation about z)
+    and the time step it ended with."""
+    d = np.load(path)
+    th = d["theta"].astype(np.float64)
+    n = th.size
+    cells = {"x": d["x"].astype(np.float64), "y": d["y"].astype(np.float64), "z": np.zeros(n),
+             "q0": np.cos(th / 2), "q1": np.zeros(n), "q2": np.zeros(n), "q3": np.sin(th / 2),
+             "length": d["length"].astype(np.float64), "l0": d["l0"].astype(np.float64),
+             "diameter": d["diameter"].astype(np.float64), "age": d["age"].astype(np.int32)}
+    meta = {k: d[k].tolist() for k in d.files if k not in cells and k != "theta"}
+    return cells, float(d["dt"]), meta
 
 
 def colony_jobs(n: int, rng, r_min: float, r_max: float, hard_frac: float, arrivals=None) -> list[dict]:
@@ -590,6 +625,7 @@ def main():
     ap.add_argument("--max-bbpgd", type=int, default=500000, help="BBPGD iteration cap of each job")
     ap.add_argument("--grow", action="store_true", help="grow one colony from a single cell to --radius")
     ap.add_argument("--grow-seconds", type=float, default=1500.0, help="wall-clock limit of --grow")
+    ap.add_argument("--save", default="", help="--grow: save the final colony (npz) as a benchmark start state")
     args = ap.parse_args()
     if args.grow:
         run_grow(args)
