@@ -1,21 +1,28 @@
 """Benchmark of the collision hot path: cell-steps/s of the hard model.
 
-Workload (default): one colony of radius 260 in the hard model, FP64, the
-scale of the reference's largest published run (R = 260).  The colony is a
-synthetic, deterministic dense packing (pcc_b200.synth.dense_colony: ~2.2e5
-rod cells in orientation domains, every neighbour touching), since growing a
-real one takes hours; a step is one full simulator step on it through the C
-ABI -- divide, x-sort renumbering, the ReLCP loop of contact detection and
-BBPGD solves, motion, growth and the CFL time-step adaptation (dt starts at
-3e-4, capped at 1e-3).  value = sum of cells over the K timed steps / device
-time (CUDA events on the library's stream), summed over ranks; each rank runs
-its own colony (replicas, no collective on the data path: weak scaling).
+Workload (default): config 2 -- one colony grown by this library's plain FP64
+path from a single cell to radius 260 (the reference's largest published
+run: R = 260, about 3e5 cells), stored as the start state
+proliferatingcellcollectives-idp_b200/data/colony_r260_seed0.npz (made by
+`bench.py --grow --radius 260 --precision fp64 --save ...`).  A step is one
+full simulator step on it through the C ABI -- divide, x-sort renumbering,
+the ReLCP loop of contact detection and BBPGD solves, motion, growth and
+the CFL time-step adaptation (capped at 1e-3) -- in config 2's mixed
+precision; the same steps in plain FP64 are reported beside it.  value = sum
+of cells over the K timed steps / device time (CUDA events on the library's
+stream), summed over ranks; each rank runs its own colony (replicas, no
+collective on the data path: weak scaling).  Configs 0 and 1 (hard and soft
+colonies grown from one cell to R = 20) run as whole runs after it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the reference simulator's own C++ code (compiled in
 place against single-rank PETSc/MPI stand-ins, oracle/_ref/libpccref_fast.so,
-release flags) on a bounded sample of the same workload on the host cores.
+release flags, one thread) on the same colony state.  A full reference step
+there takes minutes, so each of its steps is a bounded sample: the
+reference's own solver call with its BBPGD capped at a few iterations, whose
+time (detection, assembly, iterations) is scaled to a whole step with the
+ReLCP phases and BBPGD iterations per step that the same colony needs.
 """
 from __future__ import annotations
 
@@ -41,7 +48,8 @@ from pcc_b200 import abi, synth  # noqa: E402
 METRIC = "cell-steps/s to R_end; served colonies/s, p50/p99 vs plain GPU at same LCP tol"
 UNIT = "cell-steps/s"
 RADIUS = 260.0
-CPU_SAMPLE_RADIUS = 40.0  # bounded sample for the CPU legs (~5e3 cells)
+SNAPSHOT = ROOT / "proliferatingcellcollectives-idp_b200" / "data" / "colony_r260_seed0.npz"
+REF_SAMPLE_ITERS = (10, 30)  # BBPGD iterations of the reference's bounded samples
 # algorithmic bytes of one BBPGD iteration per constraint and per cell (the
 # mixed-precision form halves the floating-point operand terms)
 ALGO_BYTES = {"fp64": (312.0, 288.0), "mixed": (192.0, 144.0)}
@@ -129,6 +137,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def dist_backend() -> str:
+    """nccl for the replicas on GPUs; gloo (PCC_BENCH_BACKEND=gloo) for the
+    CPU test of the launch and aggregation path."""
+    return os.environ.get("PCC_BENCH_BACKEND", "nccl")
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -138,9 +152,33 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if dist_backend() == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(dist_backend(), timeout=datetime.timedelta(seconds=600))
     return world, rank, local
+
+
+def spawn_ranks(n: int) -> int:
+    """`bench.py --gpus N` without a launcher: starts N copies of this command,
+    one rank per GPU (RANK, LOCAL_RANK, WORLD_SIZE and the rendezvous on
+    127.0.0.1 in the environment), passes rank 0's output through and returns
+    the first non-zero exit status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, str(Path(__file__).resolve()), *sys.argv[1:]], env=env,
+                                      stdout=None if r == 0 else subprocess.DEVNULL))
+    rcs = [pr.wait() for pr in procs]
+    return next((rc for rc in rcs if rc), 0)
+
+
+def _tensor_device() -> str:
+    return "cuda" if dist_backend() == "nccl" else "cpu"
 
 
 def barrier(world: int):
@@ -154,7 +192,7 @@ def reduce_max(world: int, v: float) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=_tensor_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -164,9 +202,33 @@ def reduce_sum(world: int, v: float) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=_tensor_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def run_replica_selftest(args):
+    """The replica launch and aggregation without a GPU (the CPU test of the
+    --gpus N path): each rank steps its own small colony on the plain-C
+    oracle, takes a stand-in time of 100 + 50 * rank ms, and rank 0 prints the
+    whole-job line the GPU run would: cell-steps summed over ranks, time the
+    max over ranks."""
+    world, rank, _ = dist_setup()
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracles import OracleColony
+    p = abi.default_params(dt=1e-3, fixed_dt=1, seed=rank)
+    o = OracleColony(p)
+    o.set_cells(abi.seed_cell(rank))
+    cells = float(sum(o.step()["n_cells"] for _ in range(max(args.steps, 1))))
+    ms = 100.0 + 50.0 * rank
+    ms_max = reduce_max(world, ms)
+    total = reduce_sum(world, cells)
+    if rank == 0:
+        print(json.dumps({"n_gpus": world, "value": total / (ms_max / 1e3), "ms_max": ms_max,
+                          "cell_steps": total, "rank0_cell_steps": cells}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def aggregate(cells_per_rank: list[float], ms_per_rank: list[float]) -> tuple[float, float]:
@@ -175,50 +237,118 @@ def aggregate(cells_per_rank: list[float], ms_per_rank: list[float]) -> tuple[fl
     return sum(cells_per_rank) / (t / 1e3), t
 
 
-def cpu_rate(fast_ref: bool, seconds: float = 15.0, radius: float = CPU_SAMPLE_RADIUS, min_steps: int = 2,
-             max_steps: int | None = None, warmup: int = 1):
-    """cell-steps/s of a CPU implementation on a bounded sample of the workload."""
+def headline_config(n: int, radius: float, world: int, meta: dict) -> dict:
+    """The workload description both arms print (identical for the same colony)."""
+    return {"workload": f"hard model colony steps, grown colony R={radius:.0f} (config 2), mixed precision",
+            "cells": int(n), "start_state": meta.get("start_state", SNAPSHOT.name), "tolerance": 1e-3, "dt": "CFL-adaptive, cap 1e-3",
+            "ghost_mode": "single_rank", "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (state + constraints > 126 MB per step)"}
+
+
+def reference_step_model(cells: dict, dt: float, phases: float, iters: float, repeats: int = 1) -> dict:
+    """Time of one reference step on `cells`, from bounded samples of the
+    reference's own code (release build, one thread): its solver call with
+    BBPGD capped at REF_SAMPLE_ITERS iterations (the reference stops there
+    with its 'BBPGD did not converge' error); the difference of the two caps
+    gives the time per BBPGD iteration, the rest is the detection and
+    assembly of a ReLCP phase.  A step is scaled as phases x (detection +
+    assembly) + iters x (time per iteration)."""
     sys.path.insert(0, str(ROOT / "tests"))
-    from oracles import OracleColony, RefColony
-    kind = "port"
-    p = colony_params()
-    col = None
-    if fast_ref and (ROOT / "oracle" / "_ref" / "libpccref_fast.so").exists():
-        col = RefColony(p, fast=True)
-        kind = "reference"
-    else:
-        col = OracleColony(p)
-    cells = make_colony(radius, seed=0)
-    col.set_cells(cells)
-    for _ in range(warmup):
-        col.step()
-    t0 = time.perf_counter()
-    cs, k = 0.0, 0
-    while (time.perf_counter() - t0 < seconds or k < min_steps) and (max_steps is None or k < max_steps):
-        cs += col.step()["n_cells"]
-        k += 1
-    el = time.perf_counter() - t0
-    return cs / el, kind, k, len(cells["x"]), el
+    from oracles import RefColony
+    times = {j: [] for j in REF_SAMPLE_ITERS}
+    for _ in range(repeats):
+        for j in REF_SAMPLE_ITERS:
+            p = colony_params(dt=dt, max_bbpgd_iterations=j)
+            col = RefColony(p, fast=True)
+            col.set_cells(cells)
+            t0 = time.perf_counter()
+            try:
+                col.solve(dt, 1)
+            except RuntimeError:
+                pass  # stopped at the iteration cap
+            times[j].append(time.perf_counter() - t0)
+    t_lo, t_hi = (float(np.median(times[j])) for j in REF_SAMPLE_ITERS)
+    j_lo, j_hi = REF_SAMPLE_ITERS
+    t_iter = max((t_hi - t_lo) / (j_hi - j_lo), 0.0)
+    t_phase = max(t_lo - j_lo * t_iter, 0.0)
+    t_step = phases * t_phase + iters * t_iter
+    n = len(cells["x"])
+    return {"t_iteration_s": t_iter, "t_phase_s": t_phase, "t_step_s": t_step, "cell_steps_per_s": n / t_step,
+            "sampled_s": float(sum(sum(v) for v in times.values())), "phases_per_step": phases,
+            "bbpgd_iterations_per_step": iters}
+
+
+def start_state() -> tuple[dict, float, dict]:
+    """The grown R = 260 colony, or -- only if its file is missing -- the
+    synthetic dense packing of the same radius, labelled as such."""
+    if SNAPSHOT.exists():
+        return load_snapshot(str(SNAPSHOT))
+    cells = make_colony(RADIUS, seed=0)
+    return cells, 3e-4, {"radius": RADIUS, "tail_relcp": [2], "tail_bbpgd": [60],
+                         "start_state": "synthetic dense packing (grown colony file missing)"}
 
 
 def run_reference(args):
-    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    rate, kind, k, n, el = cpu_rate(True, seconds=1e9, min_steps=args.steps, max_steps=args.steps,
-                                    warmup=args.warmup)
+    cells, dt, meta = start_state()
+    n = len(cells["x"])
+    # ReLCP phases and BBPGD iterations per step of this colony, as the run that grew it measured them
+    phases = float(np.mean(meta["tail_relcp"]))
+    iters = float(np.mean(meta["tail_bbpgd"]))
+    t0 = time.perf_counter()
+    for _ in range(args.warmup):
+        reference_step_model(cells, dt, phases, iters)
+    samples = [reference_step_model(cells, dt, phases, iters) for _ in range(max(args.steps, 1))]
+    el = time.perf_counter() - t0
+    t_step = float(np.mean([m["t_step_s"] for m in samples]))
+    rate = n / t_step
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "hard model colony step, FP64 (bounded sample)", "radius": CPU_SAMPLE_RADIUS,
-                   "cells": n, "parallelism": "1 rank, 1 thread"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
-                         "sample": f"{k} steps of the synthetic dense colony at R={CPU_SAMPLE_RADIUS:g} "
-                                   f"({n} cells) after {args.warmup} warm-up steps"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (colony grown by this library)",
+        "config": headline_config(n, meta["radius"], world, meta),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"each step a bounded sample on the same R={meta['radius']:.0f} colony ({n} "
+                                   f"cells): the reference's solver call with BBPGD capped at "
+                                   f"{REF_SAMPLE_ITERS[0]} and {REF_SAMPLE_ITERS[1]} iterations, scaled to "
+                                   f"{phases:.1f} ReLCP phases and {iters:.0f} BBPGD iterations per step (the "
+                                   f"colony's own counts); {samples[-1]['t_iteration_s'] * 1e3:.1f} ms per BBPGD "
+                                   f"iteration, {samples[-1]['t_phase_s']:.2f} s per phase of detection and "
+                                   f"assembly; release build, one rank, one thread; {el:.0f} s sampled"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def timed_steps(col, stream, steps: int, verbose: bool = False):
+    """K steps of a colony between two CUDA events on its stream."""
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hist = []
+    e0.record(stream)
+    for _ in range(steps):
+        hist.append(col.step())
+        if verbose:
+            print(json.dumps(hist[-1]), file=sys.stderr, flush=True)
+    e1.record(stream)
+    e1.synchronize()
+    return hist, e0.elapsed_time(e1)
+
+
+def roofline(prof: dict, precision: str, peaks: dict) -> dict:
+    bb_ms = prof["bbpgd_ms"]
+    achieved = prof["bbpgd_algo_bytes"] / (bb_ms / 1e3) / 1e9 if bb_ms > 0 else 0.0
+    mixed = precision == "mixed"
+    ratio = traffic_ratio("k_bbpgd_planar_mixed_frozen_r260" if mixed else "k_bbpgd_planar_frozen_r260")
+    launches_bb = max(prof["bbpgd_launches"], 1)
+    return {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
+            "traffic": ratio * prof["bbpgd_algo_bytes"] / launches_bb if ratio else None,
+            "kernel": f"k_bbpgd_planar<{'float' if mixed else 'double'}> (persistent BBPGD)",
+            "peak_source": "fallback" if peaks.get("fallback") else "measured"}
 
 
 def run_ours(args):
@@ -229,41 +359,37 @@ def run_ours(args):
     barrier(world)
     import torch
     torch.cuda.init()
-    cells = make_colony(args.radius, seed=rank)
-    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
-    p = colony_params(capacity_hint=int(len(cells["x"]) * 1.5), precision=prec)
-    col = device.Colony(p, device=local)
-    col.set_cells(cells)
-    stream = torch.cuda.ExternalStream(col.stream, device=f"cuda:{local}")
+    cells, dt0, meta = start_state()
+    n0 = len(cells["x"])
+    peaks = measured_peaks()
+
+    def colony(precision: int):
+        p = colony_params(dt=dt0, capacity_hint=int(n0 * 1.2), precision=precision)
+        c = device.Colony(p, device=local)
+        c.set_cells(cells)
+        return c, p, torch.cuda.ExternalStream(c.stream, device=f"cuda:{local}")
+
+    # ---- headline: config 2 in mixed precision
+    col, p, stream = colony(abi.PRECISION_MIXED)
     for _ in range(args.warmup):
         col.step()
-    errors = precision_errors(device, col, p, local) if rank == 0 and prec == abi.PRECISION_MIXED else None
+    errors = precision_errors(device, col, p, local) if rank == 0 else None
     col.profiling(True)
     launches0 = col.launches
     barrier(world)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    hist = []
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            hist.append(col.step())
-            if args.verbose:
-                print(json.dumps(hist[-1]), file=sys.stderr, flush=True)
-        e1.record(stream)
-        e1.synchronize()
-    torch.cuda.synchronize()
+        hist, ms = timed_steps(col, stream, args.steps, args.verbose)
     barrier(world)
-    ms = e0.elapsed_time(e1)
     launches = col.launches - launches0
     prof = col.profile()
     cells_steps = float(sum(h["n_cells"] for h in hist))
     ms_max = reduce_max(world, ms)
-    total = reduce_sum(world, cells_steps)
-    value = total / (ms_max / 1e3)
+    value = reduce_sum(world, cells_steps) / (ms_max / 1e3)
+    iters_step = prof["bbpgd_iterations"] / max(args.steps, 1)
+    phases_step = float(np.mean([h["relcp_iterations"] for h in hist])) if hist else 0.0
 
-    # end to end through the C ABI with host buffers: upload the state from
-    # pinned host memory, step, read the state back, every step
+    # ---- end to end through the C ABI with host buffers: upload the state
+    # from pinned host memory, step, read the state back, every step
     n_cap = int(hist[-1]["n_cells"] * 1.3) + 16
     host = {f: torch.empty(n_cap, dtype=torch.float64, pin_memory=True) for f in abi.CELL_FIELDS}
     host["age"] = torch.empty(n_cap, dtype=torch.int32, pin_memory=True)
@@ -300,59 +426,102 @@ def run_ours(args):
     t1.synchronize()
     barrier(world)
     e2e_ms = reduce_max(world, t0.elapsed_time(t1))
-    e2e_total = reduce_sum(world, e2e_cells)
-    e2e_value = e2e_total / (e2e_ms / 1e3)
+    e2e_value = reduce_sum(world, e2e_cells) / (e2e_ms / 1e3)
+    col.close()
 
-    peaks = measured_peaks()
-    bb_ms = prof["bbpgd_ms"]
-    achieved = prof["bbpgd_algo_bytes"] / (bb_ms / 1e3) / 1e9 if bb_ms > 0 else 0.0
-    mixed = prec == abi.PRECISION_MIXED
-    ratio = traffic_ratio("k_bbpgd_planar_mixed_frozen_r260" if mixed else "k_bbpgd_planar_frozen_r260")
-    launches_bb = max(prof["bbpgd_launches"], 1)
-    traffic = ratio * prof["bbpgd_algo_bytes"] / launches_bb if ratio else None
+    # ---- the same steps in plain FP64 (the north star's plain method)
+    col64, p64, stream64 = colony(abi.PRECISION_FP64)
+    for _ in range(args.warmup):
+        col64.step()
+    col64.profiling(True)
+    barrier(world)
+    hist64, ms64 = timed_steps(col64, stream64, args.steps)
+    barrier(world)
+    prof64 = col64.profile()
+    ms64_max = reduce_max(world, ms64)
+    value64 = reduce_sum(world, float(sum(h["n_cells"] for h in hist64))) / (ms64_max / 1e3)
+    final64 = col64.get_cells() if rank == 0 else None
+    col64.close()
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if prec == abi.PRECISION_FP64 else "f32 operands / f64 accumulation",
-        "data": "synthetic",
-        "config": {"workload": f"hard model colony step, {'FP64' if prec == abi.PRECISION_FP64 else 'mixed precision'}"
-                               f", synthetic dense colony R={args.radius:g}",
-                   "cells_per_rank": int(hist[0]["n_cells"]), "ghost_mode": "single_rank",
-                   "tolerance": p.tolerance, "dt_start": 3e-4, "dt_cap": 1e-3,
-                   "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (state + constraints > 126 MB per step)"},
-        "roofline": {"bound": "hbm", "achieved": achieved,
-                     "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
-                     "traffic": traffic,
-                     "kernel": f"k_bbpgd_planar<{'float' if mixed else 'double'}> (persistent BBPGD)",
-                     "peak_source": "fallback" if peaks.get("fallback") else "measured"},
+        "vs_baseline": None, "dtype": "f32 operands / f64 accumulation",
+        "data": "synthetic (colony grown by this library from one cell)",
+        "config": headline_config(n0, meta["radius"], world, meta),
+        "roofline": roofline(prof, "mixed", peaks),
         "bbpgd_iterations_per_s": prof["bbpgd_iterations"] / (ms / 1e3),
-        "bbpgd_iterations_per_step": prof["bbpgd_iterations"] / max(args.steps, 1),
-        "stage_ms": {"bbpgd": bb_ms, "detect": prof["detect_ms"], "solve": prof["solve_ms"], "total": ms},
+        "bbpgd_iterations_per_step": iters_step, "relcp_phases_per_step": phases_step,
+        "bbpgd_iterations_per_step_thesis_r260": 7800,
+        "stage_ms": {"bbpgd": prof["bbpgd_ms"], "detect": prof["detect_ms"], "solve": prof["solve_ms"], "total": ms},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
                 "d2h_bytes_per_step": d2h // e2e_steps},
         "gpu_launches": launches,
         "clocks": clk.summary(),
+        "fp64": {"value": value64, "ms_per_step": ms64_max / args.steps,
+                 "bbpgd_iterations_per_step": prof64["bbpgd_iterations"] / max(args.steps, 1),
+                 "roofline": roofline(prof64, "fp64", peaks)},
     }
+    if final64 is not None:
+        line["packing_fraction"] = packing_fraction(final64)
     if errors is not None:
         line["mixed_vs_fp64"] = errors
     if rank == 0 and world == 1 and not args.no_cpu:
-        # one step of the same colony (~20 s of CPU work at R = 260): the first
-        # step from the packing, FP64, the reference's own code at release flags
-        rate, kind, k, ncpu, el = cpu_rate(True, seconds=0.0, radius=args.radius, min_steps=1, max_steps=1,
-                                           warmup=0)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
-                                "sample": f"{k} step ({el:.1f} s) of the same synthetic dense colony at "
-                                          f"R={args.radius:g} ({ncpu} cells), the first step from the packing, "
-                                          f"FP64; one rank, one thread (the reference has no threaded path "
-                                          f"and no MPI is available)"}
+        ref = reference_step_model(cells, dt0, phases_step, iters_step)
+        line["cpu_baseline"] = {
+            "value": ref["cell_steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"the reference's solver call (release build, one thread) on the same R={meta['radius']:.0f} "
+                      f"colony with BBPGD capped at {REF_SAMPLE_ITERS[0]} and {REF_SAMPLE_ITERS[1]} iterations "
+                      f"({ref['sampled_s']:.0f} s): {ref['t_iteration_s'] * 1e3:.1f} ms per BBPGD iteration, "
+                      f"{ref['t_phase_s']:.2f} s per ReLCP phase of detection and assembly, scaled to the "
+                      f"{phases_step:.1f} phases and {iters_step:.0f} iterations per step of the timed GPU steps",
+            "bbpgd_iterations_per_s": 1.0 / ref["t_iteration_s"] if ref["t_iteration_s"] > 0 else None}
+    if rank == 0 and not args.no_small:
+        line["config0"] = grow_small(device, local, soft=False)
+        line["config1"] = grow_small(device, local, soft=True)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    col.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def grow_small(device, local: int, soft: bool) -> dict:
+    """Configs 0 and 1 as whole runs: one colony grown from a single cell
+    (orientation from seed 0) to R = 20 -- hard model, FP64, dt = 1e-3 fixed;
+    or soft model, dt = 3e-5, kcc = 4/3 E (E = 1e3, R_eff = 0.125) -- timed
+    with CUDA events; for the soft colony also config 1's microbench, the force
+    and torque assembly on its final state repeated 1e4 times, with its
+    roofline on 104 B per contact and 56 B per cell."""
+    import torch
+    if soft:
+        p = abi.default_params(dt=3e-5, fixed_dt=1, seed=0, mode=abi.MODE_SOFT, kcc=1333.3333333333333)
+    else:
+        p = abi.default_params(dt=1e-3, fixed_dt=1, seed=0, mode=abi.MODE_HARD)
+    col = device.Colony(p, device=local)
+    col.set_cells(abi.seed_cell(0))
+    stream = torch.cuda.ExternalStream(col.stream, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(stream)
+    steps, cell_steps, st = col.run(20.0, 10**7)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"workload": ("soft" if soft else "hard") + " colony grown from one cell to R=20",
+           "steps": steps, "cells": st["n_cells"], "cell_steps_per_s": cell_steps / (ms / 1e3),
+           "device_s": ms / 1e3, "wall_s": time.time() - w0, "us_per_step": ms * 1e3 / max(steps, 1)}
+    if soft:
+        reps = 10000
+        t = col.soft_forces_frozen(reps)
+        m = col.detect(0.0)["sd"].size
+        algo = 104.0 * m + 56.0 * st["n_cells"]
+        out["frozen_assembly"] = {"repeats": reps, "contacts": m, "us_per_assembly": t * 1e3,
+                                  "algo_gbs": algo / (t / 1e3) / 1e9,
+                                  "frac_of_hbm": algo / (t / 1e3) / 1e9 / measured_peaks()["hbm_gbs"]}
+    col.close()
+    return out
 
 
 def packing_fraction(c: dict) -> float:
@@ -608,6 +777,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--radius", type=float, default=RADIUS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-small", action="store_true", help="skip the config 0 / config 1 runs")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="BBPGD operand precision (mixed: FP32 D/L/M/U, FP64 gamma, dots, residual)")
     ap.add_argument("--verbose", action="store_true", help="per-step solver statistics on stderr")
@@ -626,8 +796,13 @@ def main():
     ap.add_argument("--grow", action="store_true", help="grow one colony from a single cell to --radius")
     ap.add_argument("--grow-seconds", type=float, default=1500.0, help="wall-clock limit of --grow")
     ap.add_argument("--save", default="", help="--grow: save the final colony (npz) as a benchmark start state")
+    ap.add_argument("--replica-selftest", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
-    if args.grow:
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
+    if args.replica_selftest:
+        run_replica_selftest(args)
+    elif args.grow:
         run_grow(args)
     elif args.jobs > 0 or args.rate > 0:
         run_jobs(args)

@@ -66,3 +66,25 @@ def test_replicas_aggregate_over_two_ranks():
     assert v0 == pytest.approx((cells0 + cells1) / 0.150)
     assert m0 == m1 == 150.0
     assert cells0 > 800 and cells1 > 800          # both replicas divided
+
+
+def test_bench_starts_its_own_ranks():
+    """`bench.py --gpus 2` without a launcher starts two ranks itself (the
+    rendezvous on 127.0.0.1), and rank 0 reports the whole-job figure: the
+    cell-steps of both replicas over the slowest rank's time (gloo here, NCCL
+    on GPUs)."""
+    import json
+    import subprocess
+
+    env = dict(os.environ, PCC_BENCH_BACKEND="gloo")
+    env.pop("WORLD_SIZE", None)
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--steps", "700",
+                        "--replica-selftest"], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    out = lines[0]
+    assert out["n_gpus"] == 2
+    assert out["ms_max"] == 150.0
+    assert out["cell_steps"] > out["rank0_cell_steps"] >= 700
+    assert out["value"] == pytest.approx(out["cell_steps"] / 0.150)
