@@ -131,7 +131,13 @@ void profile_detect(pcc_ctx* ctx) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
   } while (0)
 
-pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
+// The ReLCP loop (Hard.cpp:91-192).  Host round trips: the detection pass of
+// each phase synchronises once (twice when it rebins); the largest overlap of
+// the earlier phases' constraints and the previous BBPGD launch's scalars ride
+// on that synchronisation instead of waiting on their own.  end_check: read
+// the device status before returning (a step defers it to its own single
+// end-of-step synchronisation).
+pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st, bool end_check) {
   const double tol = ctx->params.tolerance;
   int phase = 0;
   // BBPGD trace on every 10th step (dynamics/models/Hard.cpp:107-111); a new
@@ -144,17 +150,37 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
   long long total_it = 0;
   double res = 0.0, max_ov = 0.0;
   ctx->ncons = 0;
+  ctx->bbpgd_pending = false;
   CU(reset_ldot(ctx), "reset");
   CU(mobility(ctx), "mobility");
   // U_ext: Brownian kicks at ReLCP phase 0 only (Hard.cpp:138-143, Physics.cpp:68)
   CU(brownian_draw(ctx), "brownian");
+  // reads the scalars of a BBPGD launch after a synchronisation point
+  auto collect = [&]() -> pcc_status {
+    if (!ctx->bbpgd_pending) return PCC_OK;
+    long long it = 0;
+    int status = 0;
+    bbpgd_collect(ctx, &it, &res, &status);
+    total_it += it;
+    if (status == PCC_ERR_NOCONV_BBPGD) return fail(ctx, status, "BBPGD did not converge");
+    if (status) {
+      pcc_status dev = check_device(ctx, "bbpgd");
+      return dev ? dev : fail(ctx, status, "BBPGD device error");
+    }
+    return PCC_OK;
+  };
   while ((long long)phase < ctx->params.max_recursive_iterations) {
     const size_t before = ctx->ncons;
-    double ov_old = 0.0, ov_new = 0.0;
-    if (before) CU(max_overlap(ctx, 0, before, &ov_old), "max_overlap");
+    if (before) CU(max_overlap_enqueue(ctx, 0, before), "max_overlap");
     size_t added = 0;
+    double ov_new = 0.0;
     if (ctx->profiling) cudaEventRecord(ctx->ev[2], ctx->stream);
     CU(detect_contacts(ctx, phase == 0 ? .25 : tol, phase, phase > 0, &added, &ov_new), "detect");
+    if (ctx->n == 0) CU(cudaStreamSynchronize(ctx->stream), "detect");  // an empty colony's detection did not wait
+    pcc_status rc = collect();  // the previous phase's BBPGD, now complete
+    if (rc) return rc;
+    double ov_old = 0.0;
+    if (before) std::memcpy(&ov_old, ctx->pinned_ll + kSlotMaxOld, sizeof ov_old);
     max_ov = ov_old < ov_new ? ov_new : ov_old;
     if (max_ov <= tol && phase > 0) {
       profile_detect(ctx);
@@ -162,19 +188,26 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
     }
     CU(build_incidence(ctx), "incidence");
     profile_detect(ctx);
+    ctx->trace_phase = phase;
     long long it = 0;
     int status = 0;
-    ctx->trace_phase = phase;
-    CU(bbpgd_solve(ctx, dt, &it, &res, &status), "bbpgd");
+    CU(bbpgd_solve(ctx, dt, &it, &res, &status, /*defer=*/true), "bbpgd");
     ctx->uext_active = false;
-    total_it += it;
-    if (status == PCC_ERR_NOCONV_BBPGD) return fail(ctx, status, "BBPGD did not converge");
-    if (status) {
-      pcc_status dev = check_device(ctx, "bbpgd");
-      return dev ? dev : fail(ctx, status, "BBPGD device error");
+    if (!ctx->bbpgd_pending) {  // a traced solve synchronised and was read already
+      total_it += it;
+      if (status == PCC_ERR_NOCONV_BBPGD) return fail(ctx, status, "BBPGD did not converge");
+      if (status) {
+        pcc_status dev = check_device(ctx, "bbpgd");
+        return dev ? dev : fail(ctx, status, "BBPGD device error");
+      }
     }
     CU(apply_hard_solution(ctx, dt), "move");
     ++phase;
+  }
+  if (ctx->bbpgd_pending) {  // the loop ran out of phases right after a solve
+    CU(cudaStreamSynchronize(ctx->stream), "bbpgd");
+    pcc_status rc = collect();
+    if (rc) return rc;
   }
   if (ctx->trace_active) {
     ctx->trace_active = false;
@@ -184,8 +217,10 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
       return fail(ctx, PCC_ERR_INVALID, "cannot write the BBPGD trace files");
   }
   CU(grow_cells(ctx, dt), "grow");
-  pcc_status rc = check_device(ctx, "hard step");
-  if (rc) return rc;
+  if (end_check) {
+    pcc_status rc = check_device(ctx, "hard step");
+    if (rc) return rc;
+  }
   if (st) {
     st->relcp_iterations = phase;
     st->bbpgd_iterations = total_it;
@@ -199,7 +234,7 @@ pcc_status solve_hard(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* st) {
   return PCC_OK;
 }
 
-pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
+pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st, bool end_check) {
   ctx->ncons = 0;
   CU(reset_ldot(ctx), "reset");
   CU(brownian_draw(ctx), "brownian");  // Soft.cpp:94
@@ -212,8 +247,10 @@ pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
   CU(soft_forces_and_move(ctx, dt), "soft");
   ctx->uext_active = false;
   CU(grow_cells(ctx, dt), "grow");
-  pcc_status rc = check_device(ctx, "soft step");
-  if (rc) return rc;
+  if (end_check) {
+    pcc_status rc = check_device(ctx, "soft step");
+    if (rc) return rc;
+  }
   if (st) {
     st->relcp_iterations = 0;
     st->bbpgd_iterations = 0;
@@ -223,6 +260,29 @@ pcc_status solve_soft(pcc_ctx* ctx, double dt, pcc_step_stats* st) {
     st->n_cells = (long long)ctx->n;
   }
   return PCC_OK;
+}
+
+// One solver call (ParticleManager::step).
+pcc_status solve(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* out, bool end_check) {
+  pcc_step_stats st;
+  std::memset(&st, 0, sizeof st);
+  ctx->div_known = false;  // lengths change
+  if (ctx->profiling) cudaEventRecord(ctx->ev[4], ctx->stream);
+  if (ctx->n) CU(cudaMemsetAsync(ctx->cells.ncons.p, 0, ctx->n * sizeof(int), ctx->stream), "reset");  // Particle::reset
+  pcc_status rc = ctx->params.mode == PCC_MODE_SOFT ? solve_soft(ctx, dt, &st, end_check)
+                                                    : solve_hard(ctx, dt, iter, &st, end_check);
+  st.dt_used = dt;
+  if (ctx->profiling) {
+    cudaEventRecord(ctx->ev[5], ctx->stream);
+    cudaEventSynchronize(ctx->ev[5]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+    ctx->prof.solve_ms += ms;
+    ctx->prof.solves++;
+    ctx->prof.cell_solves += (double)st.n_cells;
+  }
+  if (out) *out = st;
+  return rc;
 }
 
 pcc_status download_contacts(pcc_ctx* ctx, size_t m, pcc_contacts* o) {
@@ -308,6 +368,7 @@ pcc_status pcc_create(const pcc_params* params, int device, pcc_ctx** out) {
   if (!e) e = cudaMallocAsync(&ctx->status, sizeof(DevStatus), ctx->stream);
   if (!e) e = cudaMallocHost(&ctx->status_host, sizeof(DevStatus));
   if (!e) e = cudaMallocHost(&ctx->pinned_ll, 64 * sizeof(long long));
+  if (!e) e = cudaMallocHost(&ctx->scal_host, sizeof(SolverScalars));
   if (!e) e = cudaMemsetAsync(ctx->status, 0, sizeof(DevStatus), ctx->stream);
   if (!e && params->capacity_hint > 0) e = ctx->cells.reserve((size_t)params->capacity_hint, 0, ctx->stream);
   if (!e) e = cudaStreamSynchronize(ctx->stream);
@@ -335,6 +396,7 @@ pcc_status pcc_destroy(pcc_ctx* ctx) {
   if (ctx->status) cudaFreeAsync(ctx->status, ctx->stream);
   if (ctx->status_host) cudaFreeHost(ctx->status_host);
   if (ctx->pinned_ll) cudaFreeHost(ctx->pinned_ll);
+  if (ctx->scal_host) cudaFreeHost(ctx->scal_host);
   if (ctx->brown_host) cudaFreeHost(ctx->brown_host);
   cudaStream_t s = ctx->stream;
   delete ctx;  // device buffers are freed on the context's stream
@@ -399,6 +461,7 @@ pcc_status pcc_upload_cells(pcc_ctx* ctx, const pcc_cells* c, size_t n) {
   if (n) cudaMemsetAsync(v.ncons, 0, n * sizeof(int), s);
   ctx->n = n;
   ctx->ncons = 0;
+  ctx->div_known = false;
   CU(cudaStreamSynchronize(s), "upload");
   CU(colony_radius(ctx, &ctx->radius), "radius");
   return PCC_OK;
@@ -445,25 +508,13 @@ pcc_status pcc_download_cells(pcc_ctx* ctx, pcc_cells* c, size_t cap, size_t* n)
 pcc_status pcc_solve(pcc_ctx* ctx, double dt, int iter, pcc_step_stats* out) {
   if (!ctx || !(dt > 0)) return PCC_ERR_INVALID;
   cudaSetDevice(ctx->device);
-  pcc_step_stats st;
-  std::memset(&st, 0, sizeof st);
-  if (ctx->profiling) cudaEventRecord(ctx->ev[4], ctx->stream);
-  if (ctx->n) CU(cudaMemsetAsync(ctx->cells.ncons.p, 0, ctx->n * sizeof(int), ctx->stream), "reset");  // Particle::reset
-  pcc_status rc = ctx->params.mode == PCC_MODE_SOFT ? solve_soft(ctx, dt, &st) : solve_hard(ctx, dt, iter, &st);
-  st.dt_used = dt;
-  if (ctx->profiling) {
-    cudaEventRecord(ctx->ev[5], ctx->stream);
-    cudaEventSynchronize(ctx->ev[5]);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
-    ctx->prof.solve_ms += ms;
-    ctx->prof.solves++;
-    ctx->prof.cell_solves += (double)st.n_cells;
-  }
-  if (out) *out = st;
-  return rc;
+  return solve(ctx, dt, iter, out, /*end_check=*/true);
 }
 
+// One Domain::run iteration (Domain.cpp:125-153).  The end-of-step work --
+// the device status, the adaptDt median, the colony radius and the division
+// count of the next step -- comes back in one copy after one synchronisation;
+// the next step's divisions use that count without waiting again.
 pcc_status pcc_step(pcc_ctx* ctx, pcc_step_stats* out) {
   if (!ctx) return PCC_ERR_INVALID;
   cudaSetDevice(ctx->device);
@@ -473,17 +524,31 @@ pcc_status pcc_step(pcc_ctx* ctx, pcc_step_stats* out) {
   CU(divide_cells(ctx, &added), "divide");
   CU(sort_cells_by_x(ctx), "sort");
   const double dt = ctx->params.dt;
-  pcc_status rc = pcc_solve(ctx, dt, (int)ctx->iter, &st);
+  pcc_status rc = solve(ctx, dt, (int)ctx->iter, &st, /*end_check=*/false);
   if (rc) {
     if (out) *out = st;
     return rc;
   }
   ctx->sim_time += dt;
+  if (!ctx->params.fixed_dt) CU(adapt_dt_enqueue(ctx), "adapt_dt");
+  CU(radius_enqueue(ctx), "radius");
+  CU(division_count_enqueue(ctx), "divide");
+  CU(cudaMemcpyAsync(ctx->status_host, ctx->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, ctx->stream), "step");
+  CU(cudaStreamSynchronize(ctx->stream), "step");
+  if (ctx->status_host->flags) {
+    rc = check_device(ctx, ctx->params.mode == PCC_MODE_SOFT ? "soft step" : "hard step");
+    if (rc) {
+      if (out) *out = st;
+      return rc;
+    }
+  }
   if (!ctx->params.fixed_dt) {
-    CU(adapt_dt(ctx), "adapt_dt");
+    adapt_dt_collect(ctx);
     if (ctx->params.dt_cap > 0 && ctx->params.dt > ctx->params.dt_cap) ctx->params.dt = ctx->params.dt_cap;
   }
-  CU(colony_radius(ctx, &ctx->radius), "radius");
+  ctx->radius = radius_collect(ctx);
+  ctx->div_next = (size_t) * reinterpret_cast<int*>(ctx->pinned_ll + kSlotDivs);
+  ctx->div_known = true;
   ctx->iter++;
   st.n_divided = (long long)added;
   st.dt_used = dt;

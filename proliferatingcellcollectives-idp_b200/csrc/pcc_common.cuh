@@ -30,6 +30,7 @@ struct DevStatus {
   unsigned pad;
   unsigned long long drift_bits;  // largest squared displacement since the lists were built
   unsigned long long lmax_bits;   // longest cell
+  unsigned long long maxold_bits; // largest overlap of the constraints of earlier ReLCP phases
 };
 
 // Cell arrays (device pointers).

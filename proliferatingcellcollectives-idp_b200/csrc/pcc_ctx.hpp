@@ -149,6 +149,13 @@ struct pcc_ctx {
   pcc::DevBuf<int> scan_tmp;
   pcc::DevBuf<double> red;  // small reductions
 
+  // host round trips: values enqueued for the next synchronisation point
+  pcc::SolverScalars* scal_host = nullptr;  // pinned: BBPGD scalars of a launch not yet read
+  bool bbpgd_pending = false;               // a BBPGD launch whose scalars are still on their way
+  double bbpgd_pending_bytes = 0.0;         // its algorithmic bytes per iteration
+  bool div_known = false;                   // div_flag / div_off / div_next describe the resident cells
+  size_t div_next = 0;                      // divisions the next step commits
+
   pcc::DevStatus* status = nullptr;  // device
   pcc::DevStatus* status_host = nullptr;  // pinned mirror
   long long* pinned_ll = nullptr;         // pinned scratch for small read-backs

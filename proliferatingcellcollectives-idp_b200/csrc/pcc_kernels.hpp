@@ -7,6 +7,13 @@
 
 namespace pcc {
 
+// Slots of ctx->pinned_ll for values copied back at a synchronisation point
+// (slots 0..7 belong to the detection pass).
+constexpr int kSlotMedian = 8;   // two adaptDt median keys
+constexpr int kSlotRadius = 10;  // colony radius bits
+constexpr int kSlotDivs = 11;    // divisions of the next step
+constexpr int kSlotMaxOld = 12;  // largest overlap of the earlier phases' constraints
+
 // ---- pcc_scan_sort.cu
 // out[i] = sum in[0..i-1] for i in [0, n]; out has n+1 entries.
 cudaError_t exclusive_scan(pcc_ctx* ctx, const int* in, int* out, size_t n);
@@ -29,12 +36,17 @@ cudaError_t build_incidence(pcc_ctx* ctx);
 // Draws the Brownian U_ext of every cell (temperature > 0) from the context's
 // generator and sets ctx->uext_active; a no-op at temperature 0.
 cudaError_t brownian_draw(pcc_ctx* ctx);
-// One BBPGD solve on the current constraint set (hard model).
-cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* residual, int* status);
+// One BBPGD solve on the current constraint set (hard model).  With defer,
+// only launches it and enqueues the copy of its scalars (ctx->bbpgd_pending);
+// bbpgd_collect reads them after the caller's next synchronisation.
+cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* residual, int* status,
+                        bool defer = false);
+void bbpgd_collect(pcc_ctx* ctx, long long* iterations, double* residual, int* status);
+// Largest overlap of constraints [from, to) into ctx->pinned_ll[kSlotMaxOld]
+// at the next synchronisation (no host wait).
+cudaError_t max_overlap_enqueue(pcc_ctx* ctx, size_t from, size_t to);
 // Moves cells with the solver's velocities and writes back gamma / phi.
 cudaError_t apply_hard_solution(pcc_ctx* ctx, double dt);
-// Max overlap over constraints [0, ncons).
-cudaError_t max_overlap(pcc_ctx* ctx, size_t from, size_t to, double* out);
 // Soft model: Hertz forces, motion and growth parameters.
 cudaError_t soft_forces_and_move(pcc_ctx* ctx, double dt);
 // Soft model force assembly only (frozen microbench).
@@ -59,7 +71,15 @@ cudaError_t planar_bbpgd(pcc_ctx* ctx, double dt, bool mixed, const PlanarTrace&
 cudaError_t reset_ldot(pcc_ctx* ctx);
 cudaError_t grow_cells(pcc_ctx* ctx, double dt);
 // Division of every cell with len >= 2 l0, daughters appended; returns count.
+// Uses the flags counted at the end of the previous step when ctx->div_known.
 cudaError_t divide_cells(pcc_ctx* ctx, size_t* added);
+// End-of-step work whose results come back in one copy: the division flags
+// and count of the next step, the colony radius, the adaptDt median keys.
+cudaError_t division_count_enqueue(pcc_ctx* ctx);
+cudaError_t radius_enqueue(pcc_ctx* ctx);
+double radius_collect(pcc_ctx* ctx);
+cudaError_t adapt_dt_enqueue(pcc_ctx* ctx);
+void adapt_dt_collect(pcc_ctx* ctx);  // updates ctx->params.dt
 // Sort cells by x (stable) and renumber.
 cudaError_t sort_cells_by_x(pcc_ctx* ctx);
 cudaError_t colony_radius(pcc_ctx* ctx, double* out);

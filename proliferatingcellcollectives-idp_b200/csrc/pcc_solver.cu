@@ -360,7 +360,8 @@ __global__ void k_move(CellsView c, long long n, const double* __restrict__ U, c
   c.stress[i] = sig[i];
 }
 
-__global__ void k_max_overlap(const double* __restrict__ sd, long long from, long long to, DevStatus* st) {
+__global__ void k_max_overlap(const double* __restrict__ sd, long long from, long long to,
+                              unsigned long long* __restrict__ dst) {
   long long c = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double v = 0.0;
   if (c < to) v = sd[c] < 0 ? -sd[c] : 0.0;
@@ -368,7 +369,7 @@ __global__ void k_max_overlap(const double* __restrict__ sd, long long from, lon
     double w = __shfl_down_sync(0xffffffffu, v, o);
     v = v < w ? w : v;
   }
-  if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(&st->max_bits, (unsigned long long)__double_as_longlong(v));
+  if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
 }
 
 // x^1.5 correctly rounded in practice: sqrt with its exact residual and the
@@ -565,7 +566,8 @@ cudaError_t mobility(pcc_ctx* ctx) {
   return cudaGetLastError();
 }
 
-cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* residual, int* status) {
+cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* residual, int* status,
+                        bool defer) {
   cudaStream_t s = ctx->stream;
   const size_t n = ctx->n, m = ctx->ncons;
   cudaError_t e;
@@ -681,15 +683,18 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   else
     ctx->prof.bbpgd_cta_launches++;
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);
-  SolverScalars host;
-  if ((e = cudaMemcpyAsync(&host, ctx->scal.p, sizeof host, cudaMemcpyDeviceToHost, s))) return e;
+  // 312 B per constraint and 288 B per cell in FP64; the FP32 operand terms halve
+  ctx->bbpgd_pending_bytes = mixed ? 192.0 * (double)m + 144.0 * (double)n : 312.0 * (double)m + 288.0 * (double)n;
+  if ((e = cudaMemcpyAsync(ctx->scal_host, ctx->scal.p, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s))) return e;
   if ((e = cudaMemcpyAsync(ctx->status_host, ctx->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s))) return e;
+  ctx->bbpgd_pending = true;
+  if (defer && !tracing) return cudaSuccess;  // read at the caller's next synchronisation
   if ((e = cudaStreamSynchronize(s))) return e;
-  *iterations = host.iterations;
-  *residual = host.residual;
+  const long long it_done = ctx->scal_host->iterations;
+  bbpgd_collect(ctx, iterations, residual, status);
   if (tracing) {
     // records 0 .. the last iteration run (BBPGD.cpp:55-81)
-    long long nrec = host.iterations + 1;
+    long long nrec = it_done + 1;
     if (nrec > trace_cap) nrec = trace_cap;
     std::vector<double> rec((size_t)(kTraceWidth * nrec));
     if ((e = cudaMemcpy(rec.data(), ctx->trace_dev.p, rec.size() * sizeof(double), cudaMemcpyDeviceToHost)))
@@ -709,22 +714,26 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
       ctx->trace_host.push_back(t);
     }
   }
+  return cudaSuccess;
+}
+
+void bbpgd_collect(pcc_ctx* ctx, long long* iterations, double* residual, int* status) {
+  const SolverScalars& host = *ctx->scal_host;
+  ctx->bbpgd_pending = false;
+  *iterations = host.iterations;
+  *residual = host.residual;
   if (ctx->profiling) {
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     ctx->prof.bbpgd_launches++;
     ctx->prof.bbpgd_iterations += host.iterations;
     ctx->prof.bbpgd_ms += ms;
-    // 312 B per constraint and 288 B per cell in FP64; the FP32 operand terms halve
-    const double bc = mixed ? 192.0 : 312.0, bn = mixed ? 144.0 : 288.0;
-    ctx->prof.bbpgd_algo_bytes += (double)host.iterations * (bc * (double)m + bn * (double)n);
+    ctx->prof.bbpgd_algo_bytes += (double)host.iterations * ctx->bbpgd_pending_bytes;
   }
-  if (ctx->status_host->flags) {
+  if (ctx->status_host->flags)
     *status = (ctx->status_host->flags & kDevErrTimeout) ? PCC_ERR_TIMEOUT : PCC_ERR_BOUNDS;
-  } else {
+  else
     *status = host.converged ? PCC_OK : PCC_ERR_NOCONV_BBPGD;
-  }
-  return cudaSuccess;
 }
 
 cudaError_t apply_hard_solution(pcc_ctx* ctx, double dt) {
@@ -735,20 +744,16 @@ cudaError_t apply_hard_solution(pcc_ctx* ctx, double dt) {
   return cudaGetLastError();
 }
 
-cudaError_t max_overlap(pcc_ctx* ctx, size_t from, size_t to, double* out) {
+cudaError_t max_overlap_enqueue(pcc_ctx* ctx, size_t from, size_t to) {
   cudaStream_t s = ctx->stream;
-  cudaMemsetAsync(&ctx->status->max_bits, 0, sizeof(unsigned long long), s);
+  cudaMemsetAsync(&ctx->status->maxold_bits, 0, sizeof(unsigned long long), s);
   if (to > from) {
     k_max_overlap<<<grid_for((long long)(to - from)), kBlock, 0, s>>>(ctx->cons.sd.p, (long long)from, (long long)to,
-                                                                     ctx->status);
+                                                                     &ctx->status->maxold_bits);
     ctx->launches++;
   }
-  cudaMemcpyAsync(ctx->pinned_ll, &ctx->status->max_bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
-  cudaError_t e = cudaStreamSynchronize(s);
-  if (e) return e;
-  unsigned long long b = (unsigned long long)ctx->pinned_ll[0];
-  memcpy(out, &b, sizeof(double));
-  return cudaSuccess;
+  return cudaMemcpyAsync(ctx->pinned_ll + kSlotMaxOld, &ctx->status->maxold_bits, sizeof(unsigned long long),
+                         cudaMemcpyDeviceToHost, s);
 }
 
 cudaError_t soft_assemble(pcc_ctx* ctx) {

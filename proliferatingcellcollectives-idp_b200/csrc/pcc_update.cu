@@ -215,20 +215,34 @@ cudaError_t grow_cells(pcc_ctx* ctx, double dt) {
   return cudaGetLastError();
 }
 
+cudaError_t division_count_enqueue(pcc_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  const size_t n = ctx->n;
+  cudaError_t e;
+  if ((e = ctx->div_flag.reserve(n + 1, 0, s)) || (e = ctx->div_off.reserve(n + 1, 0, s))) return e;
+  if (n) {
+    k_div_flag<<<grid_for(n), kBlock, 0, s>>>(ctx->cells.len.p, ctx->cells.l0.p, (long long)n, ctx->div_flag.p);
+    ctx->launches++;
+  }
+  if ((e = exclusive_scan(ctx, ctx->div_flag.p, ctx->div_off.p, n))) return e;
+  return cudaMemcpyAsync(ctx->pinned_ll + kSlotDivs, ctx->div_off.p + n, sizeof(int), cudaMemcpyDeviceToHost, s);
+}
+
 cudaError_t divide_cells(pcc_ctx* ctx, size_t* added) {
   cudaStream_t s = ctx->stream;
   const size_t n = ctx->n;
   cudaError_t e;
   *added = 0;
   if (!n) return cudaSuccess;
-  if ((e = ctx->div_flag.reserve(n + 1, 0, s)) || (e = ctx->div_off.reserve(n + 1, 0, s))) return e;
-  k_div_flag<<<grid_for(n), kBlock, 0, s>>>(ctx->cells.len.p, ctx->cells.l0.p, (long long)n, ctx->div_flag.p);
-  ctx->launches++;
-  if ((e = exclusive_scan(ctx, ctx->div_flag.p, ctx->div_off.p, n))) return e;
-  int* pinned = reinterpret_cast<int*>(ctx->pinned_ll);
-  cudaMemcpyAsync(pinned, ctx->div_off.p + n, sizeof(int), cudaMemcpyDeviceToHost, s);
-  if ((e = cudaStreamSynchronize(s))) return e;
-  const size_t k = (size_t)pinned[0];
+  size_t k;
+  if (ctx->div_known) {  // counted at the end of the previous step, on these very cells
+    k = ctx->div_next;
+  } else {
+    if ((e = division_count_enqueue(ctx))) return e;
+    if ((e = cudaStreamSynchronize(s))) return e;
+    k = (size_t) * reinterpret_cast<int*>(ctx->pinned_ll + kSlotDivs);
+  }
+  ctx->div_known = false;
   if (!k) return cudaSuccess;
   if ((e = ctx->cells.reserve(n + k, n, s))) return e;
   k_divide<<<grid_for(n), kBlock, 0, s>>>(ctx->cells.view(), (long long)n, ctx->div_flag.p, ctx->div_off.p,
@@ -256,25 +270,37 @@ cudaError_t sort_cells_by_x(pcc_ctx* ctx) {
   return cudaGetLastError();
 }
 
-cudaError_t colony_radius(pcc_ctx* ctx, double* out) {
+cudaError_t radius_enqueue(pcc_ctx* ctx) {
   cudaStream_t s = ctx->stream;
   cudaMemsetAsync(&ctx->status->max_bits, 0, sizeof(unsigned long long), s);
   if (ctx->n) {
     k_radius<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.view(), (long long)ctx->n, ctx->status);
     ctx->launches++;
   }
-  cudaMemcpyAsync(ctx->pinned_ll, &ctx->status->max_bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
-  cudaError_t e = cudaStreamSynchronize(s);
+  return cudaMemcpyAsync(ctx->pinned_ll + kSlotRadius, &ctx->status->max_bits, sizeof(unsigned long long),
+                         cudaMemcpyDeviceToHost, s);
+}
+
+double radius_collect(pcc_ctx* ctx) {
+  double r;
+  std::memcpy(&r, ctx->pinned_ll + kSlotRadius, sizeof r);
+  return r;
+}
+
+cudaError_t colony_radius(pcc_ctx* ctx, double* out) {
+  cudaError_t e = radius_enqueue(ctx);
+  if (!e) e = cudaStreamSynchronize(ctx->stream);
   if (e) return e;
-  unsigned long long b = (unsigned long long)ctx->pinned_ll[0];
-  std::memcpy(out, &b, sizeof(double));
+  *out = radius_collect(ctx);
   return cudaSuccess;
 }
 
 // Domain::adaptDt (spatial/Domain.cpp:69-118): median of |v| + ldot (for an
 // even count, the mean of the two middle values), dt* = cfl*tol/median,
-// dt <- clamp(0.99 dt + 0.01 dt*, 0.9 dt, 1.1 dt).
-cudaError_t adapt_dt(pcc_ctx* ctx) {
+// dt <- clamp(0.99 dt + 0.01 dt*, 0.9 dt, 1.1 dt).  The enqueue half sorts the
+// speeds on the device and queues the copy of the middle keys; the collect
+// half, after the caller's synchronisation, does the host arithmetic.
+cudaError_t adapt_dt_enqueue(pcc_ctx* ctx) {
   cudaStream_t s = ctx->stream;
   const size_t n = ctx->n;
   cudaError_t e;
@@ -283,11 +309,16 @@ cudaError_t adapt_dt(pcc_ctx* ctx) {
   k_speed_keys<<<grid_for(n), kBlock, 0, s>>>(ctx->cells.view(), (long long)n, ctx->keys.p, ctx->perm.p);
   ctx->launches++;
   if ((e = radix_sort_pairs(ctx, ctx->keys.p, ctx->perm.p, n, 64))) return e;
-  unsigned long long* pk = reinterpret_cast<unsigned long long*>(ctx->pinned_ll);
   const size_t lo = n % 2 == 0 ? n / 2 - 1 : n / 2;
-  cudaMemcpyAsync(pk, ctx->keys.p + lo, 2 * sizeof(unsigned long long) - (n == 1 ? sizeof(unsigned long long) : 0),
-                  cudaMemcpyDeviceToHost, s);
-  if ((e = cudaStreamSynchronize(s))) return e;
+  return cudaMemcpyAsync(ctx->pinned_ll + kSlotMedian, ctx->keys.p + lo,
+                         2 * sizeof(unsigned long long) - (n == 1 ? sizeof(unsigned long long) : 0),
+                         cudaMemcpyDeviceToHost, s);
+}
+
+void adapt_dt_collect(pcc_ctx* ctx) {
+  const size_t n = ctx->n;
+  if (!n) return;
+  const unsigned long long* pk = reinterpret_cast<const unsigned long long*>(ctx->pinned_ll + kSlotMedian);
   double med;
   if (n % 2 == 0) {
     const double lower = key_to_double(pk[0]), upper = key_to_double(pk[1]);
@@ -296,7 +327,7 @@ cudaError_t adapt_dt(pcc_ctx* ctx) {
     med = key_to_double(pk[0]);
   }
   const double gmed = med / 1;
-  if (gmed == 0.0) return cudaSuccess;
+  if (gmed == 0.0) return;
   const double cfl = ctx->params.cfl_factor * ctx->params.tolerance;
   const double cap_dt = cfl / gmed;
   const double dt = ctx->params.dt;
@@ -306,6 +337,13 @@ cudaError_t adapt_dt(pcc_ctx* ctx) {
   const double lo_dt = 0.9 * dt, hi_dt = 1.1 * dt;
   nd = nd < lo_dt ? lo_dt : (hi_dt < nd ? hi_dt : nd);
   ctx->params.dt = nd;
+}
+
+cudaError_t adapt_dt(pcc_ctx* ctx) {
+  cudaError_t e = adapt_dt_enqueue(ctx);
+  if (!e) e = cudaStreamSynchronize(ctx->stream);
+  if (e) return e;
+  adapt_dt_collect(ctx);
   return cudaSuccess;
 }
 
