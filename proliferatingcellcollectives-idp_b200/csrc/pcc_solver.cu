@@ -398,23 +398,29 @@ __global__ void k_soft_fel(ConsView cs, long long m, const double* __restrict__ 
   fel[c] = mul(mul(R_eff, kcc), pow15(overlap));
 }
 
-// Soft model, per cell: force, torque and stress gathered over the incident
-// contacts in ascending contact order (the order of the VecSetValues ADD
-// stream for that cell), then U = M F, dC = G U and the move, growth rate.
+// Soft model, per cell: force, torque and stress summed over the incident
+// contacts -- a segmented reduction over the incidence list: kLanes lanes per
+// cell, lane l taking the cell's entries l, l + kLanes, ... in ascending
+// contact order, the lanes' sums combined by a fixed shuffle tree -- then
+// U = M F, dC = G U and the move, growth rate (first lane).
 __global__ void k_soft_cell(CellsView c, long long n, ConsView cs, const int* __restrict__ inc_off,
                             const int* __restrict__ inc_ent, const double* __restrict__ fel, double xi, double lambda,
                             double tau, double dt, int move, const double* __restrict__ uext) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int gl = (int)(t % kLanes);
+  const long long i = t / kLanes;
+  // every lane of a group takes part in the shuffles: the group's cell is past
+  // the end only for whole groups, which return together
   if (i >= n) return;
   double F[6] = {0, 0, 0, 0, 0, 0};
   double sg = 0.0;
-  for (int k = inc_off[i]; k < inc_off[i + 1]; ++k) {
+  for (int k = inc_off[i] + gl; k < inc_off[i + 1]; k += kLanes) {
     const int ent = inc_ent[k];
     const long long q = ent >> 1;
     if (-cs.sd[q] <= 0.00) continue;  // Soft.cpp:49 skips non-overlapping contacts
     const double fe = fel[q];
     const double fi[3] = {mul(cs.nx[q], fe), mul(cs.ny[q], fe), mul(cs.nz[q], fe)};
-    double f[3], r[3], t[3];
+    double f[3], r[3];
     if ((ent & 1) == 0) {
       f[0] = fi[0];
       f[1] = fi[1];
@@ -430,11 +436,21 @@ __global__ void k_soft_cell(CellsView c, long long n, ConsView cs, const int* __
       r[1] = cs.rjy[q];
       r[2] = cs.rjz[q];
     }
-    cross3(r, f, t);
+    double tq[3];
+    cross3(r, f, tq);
     for (int d = 0; d < 3; ++d) F[d] = add(F[d], f[d]);
-    for (int d = 0; d < 3; ++d) F[3 + d] = add(F[3 + d], t[d]);
+    for (int d = 0; d < 3; ++d) F[3 + d] = add(F[3 + d], tq[d]);
     sg = add(sg, mul((ent & 1) == 0 ? cs.si[q] : cs.sj[q], fe));
   }
+  // a group's lanes are consecutive threads of one warp (kLanes divides 32)
+  const unsigned gmask = ((1u << kLanes) - 1u) << (threadIdx.x & 31 & ~(kLanes - 1));
+#pragma unroll
+  for (int o = kLanes / 2; o > 0; o >>= 1) {
+#pragma unroll
+    for (int d = 0; d < 6; ++d) F[d] = add(F[d], __shfl_xor_sync(gmask, F[d], o));
+    sg = add(sg, __shfl_xor_sync(gmask, sg, o));
+  }
+  if (gl != 0) return;
   if (!move) {
     for (int d = 0; d < 6; ++d) c.force[6 * i + d] = F[d];
     c.stress[i] = sg;
@@ -767,9 +783,9 @@ cudaError_t soft_assemble(pcc_ctx* ctx) {
     ctx->launches++;
   }
   if (ctx->n) {
-    k_soft_cell<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.view(), (long long)ctx->n, ctx->cons.view(),
-                                                    ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p, ctx->params.xi,
-                                                    ctx->params.lambda, ctx->params.tau, 0.0, 0, nullptr);
+    k_soft_cell<<<grid_for((long long)ctx->n * kLanes), kBlock, 0, s>>>(
+        ctx->cells.view(), (long long)ctx->n, ctx->cons.view(), ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p,
+        ctx->params.xi, ctx->params.lambda, ctx->params.tau, 0.0, 0, nullptr);
     ctx->launches++;
   }
   return cudaGetLastError();
@@ -786,10 +802,9 @@ cudaError_t soft_forces_and_move(pcc_ctx* ctx, double dt) {
     ctx->launches++;
   }
   if (ctx->n) {
-    k_soft_cell<<<grid_for(ctx->n), kBlock, 0, s>>>(ctx->cells.view(), (long long)ctx->n, ctx->cons.view(),
-                                                    ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p, ctx->params.xi,
-                                                    ctx->params.lambda, ctx->params.tau, dt, 1,
-                                                    ctx->uext_active ? ctx->uext.p : nullptr);
+    k_soft_cell<<<grid_for((long long)ctx->n * kLanes), kBlock, 0, s>>>(
+        ctx->cells.view(), (long long)ctx->n, ctx->cons.view(), ctx->inc_off.p, ctx->inc_ent.p, ctx->fel.p,
+        ctx->params.xi, ctx->params.lambda, ctx->params.tau, dt, 1, ctx->uext_active ? ctx->uext.p : nullptr);
     ctx->launches++;
   }
   return cudaGetLastError();
