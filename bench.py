@@ -578,20 +578,24 @@ def run_frozen(args):
     phase-0 contacts once and time `--steps` solves of that constraint set
     (the captured launch of the committed ncu summaries)."""
     from pcc_b200 import device
-    cells = make_colony(args.radius, seed=0)
+    if args.start == "grown":
+        cells, dt0, _ = start_state()
+    else:
+        cells, dt0 = make_colony(args.radius, seed=0), 3e-4
     prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
-    col = device.Colony(colony_params(capacity_hint=int(len(cells["x"]) * 1.5), precision=prec))
+    col = device.Colony(colony_params(dt=dt0, capacity_hint=int(len(cells["x"]) * 1.5), precision=prec))
     col.set_cells(cells)
     for _ in range(args.warmup):
         col.step()
     n = col.n_cells
     col.profiling(True)
-    it, res, ms = col.bbpgd_frozen(3e-4, max(args.steps, 1))
+    it, res, ms = col.bbpgd_frozen(col.dt, max(args.steps, 1))
     prof = col.profile()
     bc, bn = ALGO_BYTES[args.precision]
     m = int(round((prof["bbpgd_algo_bytes"] / max(prof["bbpgd_iterations"], 1) - bn * n) / bc))
     algo = it * (bc * m + bn * n)
-    print(json.dumps({"frozen_bbpgd": True, "precision": args.precision, "radius": args.radius, "cells": n, "constraints": m, "iterations": it,
+    print(json.dumps({"frozen_bbpgd": True, "precision": args.precision, "start": args.start, "radius": args.radius,
+                      "cells": n, "constraints": m, "iterations": it, "us_per_iteration": ms * 1e3 / max(it, 1),
                       "residual": res, "ms_per_solve": ms, "algo_bytes_per_solve": algo,
                       "algo_gbs": algo / (ms / 1e3) / 1e9,
                       "frac_of_hbm": algo / (ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"]}), flush=True)
@@ -782,6 +786,8 @@ def main():
                     help="BBPGD operand precision (mixed: FP32 D/L/M/U, FP64 gamma, dots, residual)")
     ap.add_argument("--verbose", action="store_true", help="per-step solver statistics on stderr")
     ap.add_argument("--frozen", action="store_true", help="BBPGD microbench on a frozen constraint set")
+    ap.add_argument("--start", choices=["packing", "grown"], default="packing",
+                    help="--frozen: the synthetic dense packing of --radius, or the grown R=260 colony")
     ap.add_argument("--jobs", type=int, default=0, help="batch sweep of N colonies (continuous batching)")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: Poisson arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
