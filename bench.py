@@ -737,22 +737,26 @@ def run_jobs(args):
               for k, r in enumerate(res) if r["status"] != 0]
     lat = np.array([r["finish_s"] - r["arrival_s"] for r in res])
     cells = sum(r["cell_steps"] for r in res)
-    # baseline: a sample of the same jobs one at a time on the plain FP64 path
+    # baseline: a size-stratified sample of the same jobs (evenly spaced in
+    # R_end order) one at a time on the plain FP64 path
+    order = sorted(range(len(jobs)), key=lambda k: jobs[k]["end_radius"])
+    nb = min(args.baseline_jobs, len(jobs))
+    picked = sorted({order[int(round(i * (len(order) - 1) / max(nb - 1, 1)))] for i in range(nb)})
     sample = []
-    for j in jobs[: args.baseline_jobs]:
-        q = abi.Params.from_buffer_copy(j["params"])
+    for k in picked:
+        q = abi.Params.from_buffer_copy(jobs[k]["params"])
         q.precision = abi.PRECISION_FP64
-        sample.append(dict(j, params=q, arrival_s=0.0))
+        sample.append(dict(jobs[k], params=q, arrival_s=0.0))
     res1, wall1 = device.serve(sample, slots=1, hbm_budget_bytes=args.hbm_budget, check=False)
     seq_rate = sum(r["cell_steps"] for r in res1) / wall1
-    # the same jobs alone with the mix's own settings: results must be identical
+    # every sampled job alone with the mix's own settings: results must be identical
     if prec == abi.PRECISION_FP64:
         alone = res1
     else:
-        alone, _ = device.serve([dict(j, arrival_s=0.0) for j in jobs[: min(2, args.baseline_jobs)]], slots=1,
+        alone, _ = device.serve([dict(jobs[k], arrival_s=0.0) for k in picked], slots=1,
                                 hbm_budget_bytes=args.hbm_budget, check=False)
-    same = all(a["checksum"] == b["checksum"] and a["steps"] == b["steps"] and a["status"] == b["status"]
-               for a, b in zip(alone, res))
+    same = all(a["checksum"] == res[k]["checksum"] and a["steps"] == res[k]["steps"] and
+               a["status"] == res[k]["status"] for a, k in zip(alone, picked))
     line = {
         "metric": METRIC, "mode": "serve" if args.rate > 0 else "batch",
         "jobs": len(jobs), "hard_jobs": sum(j["hard"] for j in jobs), "slots": args.slots,
@@ -761,7 +765,9 @@ def run_jobs(args):
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "max": float(lat.max())},
         "one_at_a_time": {"jobs": len(sample), "cell_steps_per_s": seq_rate, "wall_s": wall1,
-                          "path": "plain FP64, one job at a time (slots = 1)"},
+                          "r_end": [jobs[k]["end_radius"] for k in picked],
+                          "path": "plain FP64, one job at a time (slots = 1), sample evenly spaced in R_end"},
+        "identity_checked_jobs": len(picked),
         "speedup_vs_one_at_a_time": (cells / wall) / seq_rate,
         "results_identical_alone_and_in_mix": same,
         "max_step_bbpgd": int(max(r["max_step_bbpgd"] for r in res)),
