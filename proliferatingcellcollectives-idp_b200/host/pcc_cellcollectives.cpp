@@ -12,7 +12,8 @@
 // -no_vtk turns the output off; -out writes the final cells as CSV.
 //
 //   pcc_cellcollectives -mode hard|soft [-dt 1e-2] [-end_radius 50] [-xi 1] [-tau 1]
-//       [-l0 1] [-lambda 1e-2] [-kcc 2e4] [-tolerance 1e-3] [-max_bbpgd_iterations 5e5]
+//       [-l0 1] [-lambda 1e-2] [-kcc 2e4] [-temperature 0] [-monolayer true]
+//       [-tolerance 1e-3] [-max_bbpgd_iterations 5e5]
 //       [-max_recursive_iterations 50] [-linked_cell_size 2.2*l0] [-cfl_factor 0.5]
 //       [-log_every_colony_radius_delta 0.5] [-log_every_sim_time_delta 1e5]
 //       [-starter_vtk path] [-no_vtk] [-precision fp64|mixed] [-log_bbgd_trace]
@@ -95,6 +96,8 @@ static void print_help(const pcc_params& p) {
   row("-l0", "Reference length", num(p.l0));
   row("-lambda", "Stress sensitivity of growth", num(p.lambda));
   row("-kcc", "Soft-model contact stiffness", num(p.kcc));
+  row("-temperature", "Simulation temperature (Brownian rotational kicks)", num(p.temperature));
+  row("-monolayer", "Brownian kicks about z only", p.monolayer ? "true" : "false");
   std::printf("\nSolver:\n");
   row("-tolerance", "BBPGD residual and ReLCP overlap tolerance", num(p.tolerance));
   row("-max_bbpgd_iterations", "BBPGD iteration cap", num((double)p.max_bbpgd_iterations));
@@ -140,6 +143,11 @@ int main(int argc, char** argv) {
   p.l0 = o.num("-l0", p.l0);
   p.lambda = o.num("-lambda", p.lambda);
   p.kcc = o.num("-kcc", p.kcc);
+  p.temperature = o.num("-temperature", p.temperature);
+  if (o.has("-monolayer")) {
+    const std::string v = o.get("-monolayer", "");
+    p.monolayer = (v.empty() || v == "1" || strcasecmp(v.c_str(), "true") == 0) ? 1 : 0;
+  }
   p.tolerance = o.num("-tolerance", p.tolerance);
   p.max_bbpgd_iterations = (long long)o.num("-max_bbpgd_iterations", (double)p.max_bbpgd_iterations);
   p.max_recursive_iterations = (long long)o.num("-max_recursive_iterations", (double)p.max_recursive_iterations);
