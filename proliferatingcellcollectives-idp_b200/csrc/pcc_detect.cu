@@ -122,23 +122,38 @@ __device__ __forceinline__ Grid grid_from(const int* bbox) {
   return g;
 }
 
+// Bin counts with warp-aggregated atomics: the lanes of a warp that fall in
+// the same bin (cells are in x-sorted order, so neighbours often do) find
+// each other with __match_any_sync and one of them adds the group's size.
 __global__ void k_bin_count(const int* __restrict__ binxyz, size_t n, const int* __restrict__ bbox,
                             int* __restrict__ key, int* __restrict__ cnt) {
-  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  Grid g = grid_from(bbox);
-  int k = ((binxyz[3 * i + 2] - g.mz) * g.ny + (binxyz[3 * i + 1] - g.my)) * g.nx + (binxyz[3 * i] - g.mx);
-  key[i] = k;
-  atomicAdd(&cnt[k], 1);
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < n;
+  int k = -1;
+  if (live) {
+    const Grid g = grid_from(bbox);
+    k = ((binxyz[3 * i + 2] - g.mz) * g.ny + (binxyz[3 * i + 1] - g.my)) * g.nx + (binxyz[3 * i] - g.mx);
+    key[i] = k;
+  }
+  const unsigned peers = __match_any_sync(0xffffffffu, k);
+  const int leader = __ffs(peers) - 1;
+  if (live && (int)(threadIdx.x & 31) == leader) atomicAdd(&cnt[k], __popc(peers));
 }
 
+// Scatter into the bins: one atomic per group of same-bin lanes reserves the
+// group's slots, each lane takes the slot of its rank in the group (the order
+// inside a bin is fixed afterwards by k_segment_sort).
 __global__ void k_bin_scatter(const int* __restrict__ key, size_t n, const int* __restrict__ off,
                               int* __restrict__ cursor, int* __restrict__ cells) {
-  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int k = key[i];
-  int pos = off[k] + atomicAdd(&cursor[k], 1);
-  cells[pos] = (int)i;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < n;
+  const int k = live ? key[i] : -1;
+  const unsigned peers = __match_any_sync(0xffffffffu, k);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  int base = 0;
+  if (live && lane == leader) base = atomicAdd(&cursor[k], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  if (live) cells[off[k] + base + __popc(peers & ((1u << lane) - 1u))] = (int)i;
 }
 
 // Sort each segment [off[s], off[s+1]) ascending (segments are short).
