@@ -24,14 +24,14 @@ constexpr int kTraceWidth = 8;  // it, residual, step size, linear, quadratic, g
 // each of 148 SMs, so every block reduces one chunk per iteration with S
 // independent constraints in flight per thread.  Nothing depends on the grid.
 constexpr int kLanes = 2;
-constexpr long long kChunkTarget = 592;
+constexpr long long kChunkTarget = 592;  // 4 blocks on each of 148 SMs
 constexpr int kMaxPerThread = 8;
-__host__ __device__ inline int chunk_per_thread(long long m) {
-  const long long s = (m + kBlock * kChunkTarget - 1) / (kBlock * kChunkTarget);
+__host__ __device__ inline int chunk_per_thread(long long m, long long target = kChunkTarget) {
+  const long long s = (m + kBlock * target - 1) / (kBlock * target);
   return s < 1 ? 1 : (s > kMaxPerThread ? kMaxPerThread : (int)s);
 }
-__host__ __device__ inline long long chunk_count(long long m) {
-  const long long per = (long long)kBlock * chunk_per_thread(m);
+__host__ __device__ inline long long chunk_count(long long m, long long target = kChunkTarget) {
+  const long long per = (long long)kBlock * chunk_per_thread(m, target);
   return (m + per - 1) / per;
 }
 constexpr int kCtaThreads = 4 * kBlock;  // one-CTA form: four 256-thread units

@@ -52,7 +52,13 @@ namespace {
 
 constexpr int kCtaCells = 1024;            // the one-CTA form up to this many cells ...
 constexpr int kCtaConstraints = 4096;      // ... and constraints
-constexpr int kMaxBlocksPerSm = 4;        // co-resident blocks per SM of the multi-block form
+// Co-resident blocks per SM of the multi-block form and the chunk target that
+// goes with it (one chunk per block per iteration), per operand precision.
+template <class Real>
+struct Occupancy {
+  static constexpr int kBlocksPerSm = 4;
+  static constexpr long long kChunks = kChunkTarget;
+};
 
 template <class Real>
 struct PT;
@@ -358,10 +364,10 @@ __device__ __forceinline__ void trace_cells(double* smt, double eq, double eg, d
   }
 }
 
-// Four blocks per SM fit the register file (64 registers a thread), which
-// the chunk sizing (kChunkTarget) assumes.
+// Occupancy<Real>::kBlocksPerSm blocks per SM fit the register file, which
+// the chunk sizing (Occupancy<Real>::kChunks) assumes.
 template <class Real, int kTr>
-__global__ void __launch_bounds__(kBlock, kTr ? 1 : 4) k_bbpgd_planar(PArgs<Real> a) {
+__global__ void __launch_bounds__(kBlock, kTr ? 1 : Occupancy<Real>::kBlocksPerSm) k_bbpgd_planar(PArgs<Real> a) {
   __shared__ double sm[4 * (kBlock / 32)];
   __shared__ double smt[kTr ? 4 * kBlock : 1];
   const int TR = kTr ? a.trace : 0;
@@ -578,7 +584,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
       (e = B::inc(ctx).reserve(ne + 1, 0, s)) || (e = B::cell(ctx).reserve(nn, 0, s)) ||
       (e = B::u(ctx).reserve(nn, 0, s)))
     return e;
-  const long long nchunks = chunk_count((long long)m);
+  const long long nchunks = chunk_count((long long)m, Occupancy<Real>::kChunks);
   if ((e = ctx->partials.reserve(4 * (nchunks + 1), 0, s))) return e;
   ConsView cv = ctx->cons.view();
   if (m) {
@@ -625,7 +631,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   a.max_it = ctx->params.max_bbpgd_iterations;
   a.partials = reinterpret_cast<double4*>(ctx->partials.p);
   a.nchunks = nchunks;
-  a.per_thread = chunk_per_thread((long long)m);
+  a.per_thread = chunk_per_thread((long long)m, Occupancy<Real>::kChunks);
   a.sc = ctx->scal.p;
   a.st_err = ctx->status;
   a.trace = tr.trace;
@@ -647,7 +653,8 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
     // at most kMaxBlocksPerSm blocks per SM: both grid barriers of an
     // iteration cost more with more arriving blocks than the extra resident
     // warps hide
-    coop = (per_sm < kMaxBlocksPerSm ? per_sm : kMaxBlocksPerSm) * ctx->num_sms;
+    const int cap = Occupancy<Real>::kBlocksPerSm;
+    coop = (per_sm < cap ? per_sm : cap) * ctx->num_sms;
   }
   long long want = (long long)grid_for((long long)n * kLanes);
   if (nchunks > want) want = nchunks;
@@ -660,7 +667,11 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
 
 }  // namespace
 
-long long planar_chunks(size_t m) { return chunk_count((long long)m); }
+long long planar_chunks(size_t m) {  // the larger of the two precisions' counts
+  const long long a = chunk_count((long long)m, Occupancy<double>::kChunks);
+  const long long b = chunk_count((long long)m, Occupancy<float>::kChunks);
+  return a > b ? a : b;
+}
 
 cudaError_t planar_bbpgd(pcc_ctx* ctx, double dt, bool mixed, const PlanarTrace& tr, int* kind) {
   return mixed ? launch<float>(ctx, dt, tr, kind) : launch<double>(ctx, dt, tr, kind);
