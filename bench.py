@@ -610,9 +610,23 @@ def run_grow(args):
     build.build()
     torch.cuda.init()
     prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
-    p = colony_params(dt=1e-3, precision=prec, capacity_hint=int(4.5 * args.radius ** 2 * 1.2) + 64)
+    done = {"steps": 0, "cell_steps": 0.0, "bbpgd": 0, "device_s": 0.0, "wall_s": 0.0, "segment": 0,
+            "stage_ms": {"bbpgd": 0.0, "detect": 0.0, "solve": 0.0}, "marks": []}
+    if args.resume:  # an earlier segment of the same run (its --checkpoint file)
+        ck = np.load(args.resume, allow_pickle=False)
+        done = json.loads(str(ck["run"]))
+        done["segment"] += 1
+    # a resumed segment draws its division lengths from its own stream (the
+    # context's position in the first stream is not part of the saved state)
+    p = colony_params(dt=1e-3, precision=prec, capacity_hint=int(4.5 * args.radius ** 2 * 1.2) + 64,
+                      seed=args.job_seed + done["segment"])
     col = device.Colony(p)
-    col.set_cells(abi.seed_cell(args.job_seed))
+    if args.resume:
+        col.set_cells({k[5:]: ck[k] for k in ck.files if k.startswith("cell_")})
+        col.dt = float(ck["dt"])
+        col.set_clock(float(ck["sim_time"]), done["steps"])
+    else:
+        col.set_cells(abi.seed_cell(args.job_seed))
     stream = torch.cuda.ExternalStream(col.stream, device="cuda:0")
     col.profiling(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -620,8 +634,8 @@ def run_grow(args):
     tlast = t0
     steps = bb = 0
     cells = 0.0
-    radius = 0.0
-    marks = []
+    radius = float(ck["radius"]) if args.resume else 0.0
+    marks = done["marks"]
     from collections import deque
     tail = deque(maxlen=50)  # solver statistics of the last steps, kept with a saved snapshot
     e0.record(stream)
@@ -633,12 +647,14 @@ def run_grow(args):
         bb += st["bbpgd_iterations"]
         radius = st["colony_radius"]
         if not marks or radius >= marks[-1]["radius"] + 20.0:
-            marks.append({"radius": radius, "step": steps, "cells": st["n_cells"], "wall_s": time.time() - t0,
-                          "dt": st["dt_used"], "bbpgd_step": st["bbpgd_iterations"]})
+            marks.append({"radius": radius, "step": done["steps"] + steps, "cells": st["n_cells"],
+                          "wall_s": done["wall_s"] + time.time() - t0, "dt": st["dt_used"],
+                          "bbpgd_step": st["bbpgd_iterations"]})
         if time.time() - tlast > 10:
             tlast = time.time()
-            print(json.dumps({"step": steps, "radius": radius, "cells": st["n_cells"], "dt": st["dt_used"],
-                              "bbpgd": st["bbpgd_iterations"], "wall_s": tlast - t0}), file=sys.stderr, flush=True)
+            print(json.dumps({"step": done["steps"] + steps, "radius": radius, "cells": st["n_cells"],
+                              "dt": st["dt_used"], "bbpgd": st["bbpgd_iterations"], "wall_s": tlast - t0}),
+                  file=sys.stderr, flush=True)
         tail.append(st)
     e1.record(stream)
     e1.synchronize()
@@ -646,15 +662,27 @@ def run_grow(args):
     dev_ms = e0.elapsed_time(e1)
     prof = col.profile()
     final = col.get_cells()
+    run = {"steps": done["steps"] + steps, "cell_steps": done["cell_steps"] + cells, "bbpgd": done["bbpgd"] + bb,
+           "device_s": done["device_s"] + dev_ms / 1e3, "wall_s": done["wall_s"] + wall, "segment": done["segment"],
+           "stage_ms": {"bbpgd": done["stage_ms"]["bbpgd"] + prof["bbpgd_ms"],
+                        "detect": done["stage_ms"]["detect"] + prof["detect_ms"],
+                        "solve": done["stage_ms"]["solve"] + prof["solve_ms"]},
+           "marks": marks}
+    if args.checkpoint:  # the exact state a next step reads (forces and velocities are recomputed), for --resume
+        np.savez_compressed(args.checkpoint, dt=np.float64(col.dt), sim_time=np.float64(st.get("sim_time", 0.0)),
+                            radius=np.float64(radius), run=np.array(json.dumps(run)),
+                            **{"cell_" + k: np.asarray(v) for k, v in final.items()
+                               if k not in ("force", "velocity", "num_constraints")})
     if args.save:
-        save_snapshot(args.save, final, col.dt, steps, st, tail, args.job_seed)
+        save_snapshot(args.save, final, col.dt, run["steps"], st, tail, args.job_seed)
     print(json.dumps({
         "grow": True, "precision": args.precision, "radius_target": args.radius, "radius": radius,
-        "reached": radius >= args.radius, "steps": steps, "cells": int(st.get("n_cells", 1)),
-        "cell_steps": cells, "wall_s": wall, "device_s": dev_ms / 1e3, "cell_steps_per_s": cells / (dev_ms / 1e3),
-        "bbpgd_iterations": bb, "bbpgd_iterations_per_s": bb / (dev_ms / 1e3),
-        "stage_ms": {"bbpgd": prof["bbpgd_ms"], "detect": prof["detect_ms"], "solve": prof["solve_ms"]},
-        "packing_fraction": packing_fraction(final), "sim_time": st.get("sim_time"), "marks": marks,
+        "reached": radius >= args.radius, "segments": run["segment"] + 1, "steps": run["steps"],
+        "cells": int(st.get("n_cells", 1)), "cell_steps": run["cell_steps"], "wall_s": run["wall_s"],
+        "device_s": run["device_s"], "cell_steps_per_s": run["cell_steps"] / run["device_s"],
+        "bbpgd_iterations": run["bbpgd"], "bbpgd_iterations_per_s": run["bbpgd"] / run["device_s"],
+        "stage_ms": run["stage_ms"], "packing_fraction": packing_fraction(final), "sim_time": st.get("sim_time"),
+        "marks": marks, "segment_steps": steps, "segment_device_s": dev_ms / 1e3,
     }), flush=True)
 
 
@@ -808,6 +836,8 @@ def main():
     ap.add_argument("--grow", action="store_true", help="grow one colony from a single cell to --radius")
     ap.add_argument("--grow-seconds", type=float, default=1500.0, help="wall-clock limit of --grow")
     ap.add_argument("--save", default="", help="--grow: save the final colony (npz) as a benchmark start state")
+    ap.add_argument("--checkpoint", default="", help="--grow: save the exact final state and run totals (npz)")
+    ap.add_argument("--resume", default="", help="--grow: continue the run saved by --checkpoint")
     ap.add_argument("--replica-selftest", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:

@@ -15,24 +15,29 @@ constexpr long long kSpinLimit = 1LL << 26;
 constexpr int kTraceWidth = 8;  // it, residual, step size, linear, quadratic, growth, total, -
 // Work decomposition shared by the general and planar solvers (identical
 // values from both): kLanes lanes per cell in the cell pass (lane l takes
-// the cell's incidence entries l, l + kLanes, ...); a reduction chunk is
-// 256 x S constraints, thread t of a 256-thread unit taking constraints
-// t, t + 256, ... of the chunk and summing its S terms in that order before
-// the unit's fixed shuffle tree.  S depends on the constraint count alone:
-// the smallest S (at most kMaxPerThread) that packs the constraints into at
-// most kChunkTarget chunks, one round of a grid of four 256-thread blocks on
-// each of 148 SMs, so every block reduces one chunk per iteration with S
-// independent constraints in flight per thread.  Nothing depends on the grid.
+// the cell's incidence entries l, l + kLanes, ...); the constraints are cut
+// into chunk_count(m) reduction chunks of nearly equal size, chunk ch
+// covering [chunk_lo(ch), chunk_lo(ch + 1)) (starts rounded down to a
+// multiple of 32, so a warp's loads start on a line), thread t of a 256-thread unit
+// taking the chunk's constraints lo + t, lo + t + 256, ... and summing its
+// terms in that order before the unit's fixed shuffle tree.  The count
+// depends on the constraint count alone: one constraint per thread while
+// that needs at most kChunkTarget chunks, else kChunkTarget chunks (one
+// round of a grid of four 256-thread blocks on each of 148 SMs, so every
+// block reduces one chunk per iteration), else as many as keep a thread at
+// kMaxPerThread constraints.  Nothing depends on the grid.
 constexpr int kLanes = 2;
 constexpr long long kChunkTarget = 592;  // 4 blocks on each of 148 SMs
 constexpr int kMaxPerThread = 8;
-__host__ __device__ inline int chunk_per_thread(long long m, long long target = kChunkTarget) {
-  const long long s = (m + kBlock * target - 1) / (kBlock * target);
-  return s < 1 ? 1 : (s > kMaxPerThread ? kMaxPerThread : (int)s);
-}
 __host__ __device__ inline long long chunk_count(long long m, long long target = kChunkTarget) {
-  const long long per = (long long)kBlock * chunk_per_thread(m, target);
-  return (m + per - 1) / per;
+  long long c = (m + kBlock - 1) / kBlock;
+  if (c > target) c = target;
+  const long long most = (long long)kBlock * kMaxPerThread;
+  if (c < (m + most - 1) / most) c = (m + most - 1) / most;
+  return c < 1 ? 1 : c;
+}
+__host__ __device__ inline long long chunk_lo(long long ch, long long m, long long nchunks) {
+  return ch >= nchunks ? m : (ch * m / nchunks) & ~31LL;
 }
 constexpr int kCtaThreads = 4 * kBlock;  // one-CTA form: four 256-thread units
 constexpr int kCtaUnits = kCtaThreads / kBlock;
@@ -235,6 +240,7 @@ __device__ __forceinline__ double bb_step(const double v[4], long long it) {
 
 // Work units.  A unit is 256 threads; chunk ch belongs to unit ch % units.
 struct GridUnits {  // the multi-block kernel: one unit per block
+  static constexpr bool kGrid = true;
   __device__ static unsigned units() { return gridDim.x; }
   __device__ static unsigned unit() { return blockIdx.x; }
   __device__ static int t() { return threadIdx.x; }
@@ -243,6 +249,7 @@ struct GridUnits {  // the multi-block kernel: one unit per block
   __device__ static long long warps() { return ((long long)gridDim.x * blockDim.x) >> 5; }
 };
 struct CtaUnits {  // the one-CTA kernel: four units in one block, each with its own named barrier
+  static constexpr bool kGrid = false;
   __device__ static unsigned units() { return kCtaUnits; }
   __device__ static unsigned unit() { return threadIdx.x / kBlock; }
   __device__ static int t() { return threadIdx.x % kBlock; }

@@ -70,6 +70,7 @@ struct ConsBufs {
 // The arrival counter sits on a cache line of its own: every block adds to
 // it at every grid barrier, while the release word and the scalars that the
 // blocks read after a release share the next line.
+constexpr int kTakeGroups = 8;
 struct SolverScalars {
   unsigned long long arrive;     // block arrivals at grid barriers, monotonic within a launch
   unsigned long long pad0[15];
@@ -80,7 +81,12 @@ struct SolverScalars {
   double alpha;                  // current step size
   double residual;               // last evaluated residual
   double res0;                   // initial residual
+  // cell-unit counters of the multi-block planar cell pass, one per 128-byte
+  // line, zeroed between passes by the barrier's reduction; not copied back
+  alignas(128) unsigned long long take[kTakeGroups][16];
 };
+constexpr size_t kScalarsCopied = offsetof(SolverScalars, take);
+static_assert(offsetof(SolverScalars, take) == 256, "counters start on their own line");
 
 }  // namespace pcc
 

@@ -18,7 +18,7 @@
 //     by a fixed shuffle tree, and the first lane forms U = M F, the growth
 //     rate and its change;
 //   constraint pass: a few constraints per thread in fixed chunks
-//     (chunk_per_thread), phi_next = Phi + dt D U - dt L dldot, the new
+//     (chunk_count, chunk_lo), phi_next = Phi + dt D U - dt L dldot, the new
 //     (gamma_k, g_k) written over the constraint's previous pair and pushed
 //     over its two incidence entries (so the next cell pass reads them in
 //     order instead of gathering), and the three Barzilai-Borwein dot
@@ -59,6 +59,8 @@ struct Occupancy {
   static constexpr int kBlocksPerSm = 4;
   static constexpr long long kChunks = kChunkTarget;
 };
+// the general (FP64) kernel cuts its chunks with the default target
+static_assert(Occupancy<double>::kChunks == kChunkTarget, "FP64 chunks must match the general kernel's");
 
 template <class Real>
 struct PT;
@@ -120,8 +122,7 @@ struct PArgs {
   double dt, lambda, tau, tol;
   long long max_it;
   double4* partials;       // one per chunk: (sum dgam^2, sum dgam*dg, sum dg^2, max residual)
-  long long nchunks;
-  int per_thread;          // constraints per thread in a chunk (chunk_per_thread(m))
+  long long nchunks;       // chunk_count(m)
   SolverScalars* sc;
   DevStatus* st_err;
   // BBPGD trace (-log_bbgd_trace), as in the general kernel
@@ -234,19 +235,43 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double
       a.imp[p] = im;
     }
   };
-  const long long stride = U::warps() * kCellsPerWarp;
-  long long p = U::warp() * kCellsPerWarp + lane / kLanes;
+  // Cell units: unit u is the cells [16 u, 16 u + 16), one per lane group of
+  // a warp.  Warp w (of W) starts with unit w; the untraced multi-block pass
+  // then draws its further units from kTakeGroups counters (warp w from
+  // counter w % kTakeGroups, whose units are W + (w % kTakeGroups) +
+  // kTakeGroups j), so blocks that run fast take more cells and the pass ends
+  // with the memory system still busy; the other forms keep the static order
+  // w, w + W, w + 2W, ...  A unit is drawn one round ahead (the first draw
+  // alongside the first unit's loads) and its cells' ranges are loaded one
+  // round ahead of their use.  Which warp does a cell changes nothing in its
+  // sums.
+  constexpr bool kDyn = !kTr && U::kGrid;
+  const long long W = U::warps(), units = (a.n + kCellsPerWarp - 1) / kCellsPerWarp;
+  const int grp = (int)(U::warp() % kTakeGroups);
+  unsigned long long* take = kDyn ? &a.sc->take[grp][0] : nullptr;
+  long long ucur = U::warp(), unext = ucur + W;
+  long long p = ucur * kCellsPerWarp + lane / kLanes;
   int b = 0, e = 0;
   V4 cl{};
   double uez = 0.0;
+  if constexpr (kDyn) {
+    unext = units;
+    if (ucur < units && lane == 0) unext = W + grp + kTakeGroups * (long long)atomicAdd(take, 1ULL);
+  }
   if (p < a.n) {
     b = a.inc_off[p];
     e = a.inc_off[p + 1];
     cl = a.cell[p];
     if (a.uext) uez = a.uext[3 * p + 2];
   }
-  for (long long pw = U::warp() * kCellsPerWarp; pw < a.n; pw += stride) {
-    const long long pn = p + stride;
+  if constexpr (kDyn) unext = __shfl_sync(kFull, unext, 0);
+  while (ucur < units) {
+    long long uafter = unext + W;
+    if constexpr (kDyn) {
+      uafter = units;
+      if (unext < units && lane == 0) uafter = W + grp + kTakeGroups * (long long)atomicAdd(take, 1ULL);
+    }
+    const long long pn = unext * kCellsPerWarp + lane / kLanes;
     int bn = 0, en = 0;
     V4 cln{};
     double uezn = 0.0;
@@ -260,6 +285,9 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double
     for (int k = b + gl; k < e; k += kLanes) accumulate(A, k);
     combine(A);
     if (gl == 0 && p < a.n) finish(p, A, cl, uez);
+    if constexpr (kDyn) uafter = __shfl_sync(kFull, uafter, 0);
+    ucur = unext;
+    unext = uafter;
     p = pn;
     b = bn;
     e = en;
@@ -270,6 +298,14 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double
 
 // phi_next of constraint c given U and dldot (MatMult row c in ascending
 // columns: gi < gj, so the i block first; VecMAXPY(phi_next, {dt, -dt}, ...)).
+// Zeroes the cell-unit counters for the next cell pass.  Called by thread 0
+// of the block that completes the second barrier of an iteration, after every
+// block has left the cell pass and before the barrier's release store.
+__device__ __forceinline__ void reset_take(SolverScalars* sc) {
+#pragma unroll
+  for (int g = 0; g < kTakeGroups; ++g) sc->take[g][0] = 0;
+}
+
 template <class Real>
 __device__ __forceinline__ double planar_grad(const PArgs<Real>& a, long long c) {
   const int2 ij = a.ij[c];
@@ -310,15 +346,12 @@ __device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, 
                                                 double* smt) {
   double2* gg = a.gg;
   double2* eout = a.ev;
-  const int S = a.per_thread;
   for (long long ch = U::unit(); ch < a.nchunks; ch += U::units()) {
     double v[4] = {0, 0, 0, 0};
     double lin = 0.0;
-    const long long base = ch * (long long)kBlock * S + U::t();
+    const long long hi = chunk_lo(ch + 1, a.m, a.nchunks);
 #pragma unroll 2
-    for (int q = 0; q < S; ++q) {
-      const long long c = base + (long long)q * kBlock;
-      if (c >= a.m) break;
+    for (long long c = chunk_lo(ch, a.m, a.nchunks) + U::t(); c < hi; c += kBlock) {
       const double2 s = gg[c];
       const double gam = mode == 0 ? s.x : project(s.x, s.y, alpha);
       const double g = planar_grad(a, c);
@@ -391,6 +424,7 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : Occupancy<Real>::kBlocksPerS
       sc->residual = v[3];
       sc->alpha = 1.0 / v[3];
       sc->converged = 0;
+      reset_take(sc);
     }
     if (TR)
       trace_record(smt, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
@@ -426,6 +460,7 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : Occupancy<Real>::kBlocksPerS
         if (!conv) sc->alpha = bb_step(v, it);
         sc->converged = conv;
         sc->iterations = it;
+        reset_take(sc);
       }
     };
     if (!bar.sync_reduce(reduce_iter)) return;
@@ -631,7 +666,6 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   a.max_it = ctx->params.max_bbpgd_iterations;
   a.partials = reinterpret_cast<double4*>(ctx->partials.p);
   a.nchunks = nchunks;
-  a.per_thread = chunk_per_thread((long long)m, Occupancy<Real>::kChunks);
   a.sc = ctx->scal.p;
   a.st_err = ctx->status;
   a.trace = tr.trace;

@@ -11,7 +11,7 @@
 //   constraint pass, one thread per constraint: phi_next = Phi + dt D U -
 //     dt L dldot, the projected-gradient residual and the three
 //     Barzilai-Borwein dot products, reduced per fixed chunk of constraints
-//     (chunk_per_thread).
+//     (chunk_count, chunk_lo).
 // The projection gamma_k = max(gamma_{k-1} - alpha g_{k-1}, 0) is recomputed
 // where it is needed (both passes), so no extra pass stores it.  The last block
 // to reach a barrier reduces the chunk partials in a fixed order and publishes
@@ -207,14 +207,11 @@ __device__ __forceinline__ void constraint_pass(const SolverArgs& a, int mode, c
                                                 double* gam_out, double* g_out, double alpha, bool check, double* sm,
                                                 double* smt) {
   double4* partials = reinterpret_cast<double4*>(a.partials);
-  const int S = chunk_per_thread(a.m);
   for (long long ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
     double v[4] = {0, 0, 0, 0};  // sum dgam^2, sum dgam*dg, sum dg^2, max residual
     double lin = 0.0;
-    const long long base = ch * (long long)kBlock * S + threadIdx.x;
-    for (int q = 0; q < S; ++q) {
-      const long long c = base + (long long)q * kBlock;
-      if (c >= a.m) break;
+    const long long hi = chunk_lo(ch + 1, a.m, a.nchunks);
+    for (long long c = chunk_lo(ch, a.m, a.nchunks) + threadIdx.x; c < hi; c += kBlock) {
       const double gpc = mode == 0 ? a.gamma[c] : ldcg(gp + c), ggc = mode == 0 ? 0.0 : ldcg(gg + c);
       const double gam = mode == 0 ? gpc : project(gpc, ggc, alpha);
       const double g = constraint_grad(a, c);
@@ -593,7 +590,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
     return e;
   if ((e = ctx->scal.reserve(1, 0, s))) return e;
   cudaMemsetAsync(ctx->scal.p, 0, sizeof(SolverScalars), s);
-  const long long nchunks = planar_chunks(m);  // the planar kernels' chunks
+  const long long nchunks = chunk_count((long long)m);  // the FP64 planar kernel's chunks
   const bool tracing = ctx->trace_active;
   long long trace_cap = 0;
   if (tracing) {
@@ -701,7 +698,7 @@ cudaError_t bbpgd_solve(pcc_ctx* ctx, double dt, long long* iterations, double* 
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], s);
   // 312 B per constraint and 288 B per cell in FP64; the FP32 operand terms halve
   ctx->bbpgd_pending_bytes = mixed ? 192.0 * (double)m + 144.0 * (double)n : 312.0 * (double)m + 288.0 * (double)n;
-  if ((e = cudaMemcpyAsync(ctx->scal_host, ctx->scal.p, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s))) return e;
+  if ((e = cudaMemcpyAsync(ctx->scal_host, ctx->scal.p, kScalarsCopied, cudaMemcpyDeviceToHost, s))) return e;
   if ((e = cudaMemcpyAsync(ctx->status_host, ctx->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s))) return e;
   ctx->bbpgd_pending = true;
   if (defer && !tracing) return cudaSuccess;  // read at the caller's next synchronisation
