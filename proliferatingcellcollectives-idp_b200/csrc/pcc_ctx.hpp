@@ -81,9 +81,9 @@ struct SolverScalars {
   double alpha;                  // current step size
   double residual;               // last evaluated residual
   double res0;                   // initial residual
-  // cell-unit counters of the multi-block planar cell pass, one per 128-byte
-  // line, zeroed between passes by the barrier's reduction; not copied back
-  alignas(128) unsigned long long take[kTakeGroups][16];
+  // cell-unit counters of the multi-block planar cell pass, two sets used by
+  // alternate iterations, one counter per 128-byte line; not copied back
+  alignas(128) unsigned long long take[2][kTakeGroups][16];
 };
 constexpr size_t kScalarsCopied = offsetof(SolverScalars, take);
 static_assert(offsetof(SolverScalars, take) == 256, "counters start on their own line");

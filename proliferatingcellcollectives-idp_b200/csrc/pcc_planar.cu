@@ -149,7 +149,7 @@ struct CellAcc {
 // flight together; each cell's sums do not depend on which group takes it.
 template <class Real, class U, int kTr>
 __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double alpha, bool final, double* eq,
-                                          double* eg) {
+                                          double* eg, int set = 0) {
   using V4 = typename PT<Real>::V4;
   constexpr bool kF64 = sizeof(Real) == 8;
   const int lane = threadIdx.x & 31, gl = lane % kLanes;
@@ -237,8 +237,8 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double
   };
   // Cell units: unit u is the cells [16 u, 16 u + 16), one per lane group of
   // a warp.  Warp w (of W) starts with unit w; the untraced multi-block pass
-  // then draws its further units from kTakeGroups counters (warp w from
-  // counter w % kTakeGroups, whose units are W + (w % kTakeGroups) +
+  // then draws its further units from kTakeGroups counters of counter set
+  // `set` (warp w from counter w % kTakeGroups, whose units are W + (w % kTakeGroups) +
   // kTakeGroups j), so blocks that run fast take more cells and the pass ends
   // with the memory system still busy; the other forms keep the static order
   // w, w + W, w + 2W, ...  A unit is drawn one round ahead (the first draw
@@ -248,7 +248,7 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double
   constexpr bool kDyn = !kTr && U::kGrid;
   const long long W = U::warps(), units = (a.n + kCellsPerWarp - 1) / kCellsPerWarp;
   const int grp = (int)(U::warp() % kTakeGroups);
-  unsigned long long* take = kDyn ? &a.sc->take[grp][0] : nullptr;
+  unsigned long long* take = kDyn ? &a.sc->take[set][grp][0] : nullptr;
   long long ucur = U::warp(), unext = ucur + W;
   long long p = ucur * kCellsPerWarp + lane / kLanes;
   int b = 0, e = 0;
@@ -298,12 +298,13 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double
 
 // phi_next of constraint c given U and dldot (MatMult row c in ascending
 // columns: gi < gj, so the i block first; VecMAXPY(phi_next, {dt, -dt}, ...)).
-// Zeroes the cell-unit counters for the next cell pass.  Called by thread 0
-// of the block that completes the second barrier of an iteration, after every
-// block has left the cell pass and before the barrier's release store.
-__device__ __forceinline__ void reset_take(SolverScalars* sc) {
+// Zeroes counter set `set` of the cell-unit counters.  Iteration k's cell
+// pass draws from set k % 2; set (k + 1) % 2 was last drawn from by iteration
+// k - 1, so one thread zeroes it between the two barriers of iteration k and
+// the second barrier orders that before iteration k + 1 draws from it.
+__device__ __forceinline__ void reset_take(SolverScalars* sc, int set) {
 #pragma unroll
-  for (int g = 0; g < kTakeGroups; ++g) sc->take[g][0] = 0;
+  for (int g = 0; g < kTakeGroups; ++g) sc->take[set][g][0] = 0;
 }
 
 template <class Real>
@@ -407,6 +408,64 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : Occupancy<Real>::kBlocksPerS
   const unsigned nb = gridDim.x;
   SolverScalars* sc = a.sc;
   GridBarrier bar{sc, a.st_err, nb};
+  if constexpr (!kTr) {
+    // Untraced: every block reduces the chunk partials itself after a plain
+    // grid barrier, in the same fixed order, so every block holds the same
+    // bits of the step size and of the convergence decision and nothing is
+    // published between blocks.  Block 0 records the scalars for the host
+    // and zeroes the cell-unit counters of the next iteration.
+    __shared__ double s_v[4];
+    auto reduce_all = [&](double v[4]) {
+      reduce_partials<GridUnits>(a.partials, a.nchunks, v, sm);
+      if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s_v[q] = v[q];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = s_v[q];
+    };
+    const bool recorder = blockIdx.x == 0 && threadIdx.x == 0;
+    cell_pass<Real, GridUnits, 0>(a, 0, 0.0, false, nullptr, nullptr, 0);
+    if (!bar.sync()) return;
+    if (recorder) reset_take(sc, 1);
+    constraint_pass<Real, GridUnits, 0>(a, 0, 0.0, true, sm, nullptr);
+    if (!bar.sync()) return;
+    double v[4];
+    reduce_all(v);
+    double alpha = 1.0 / v[3];
+    if (recorder) {
+      sc->res0 = v[3];
+      sc->residual = v[3];
+      sc->alpha = alpha;
+    }
+    long long it = 1;
+    bool conv = false;
+    while (it < a.max_it) {
+      const bool check = (it % 10) == 0;
+      cell_pass<Real, GridUnits, 0>(a, 1, alpha, check, nullptr, nullptr, (int)(it & 1));
+      if (!bar.sync()) return;
+      if (recorder) reset_take(sc, (int)((it + 1) & 1));
+      constraint_pass<Real, GridUnits, 0>(a, 1, alpha, check, sm, nullptr);
+      if (!bar.sync()) return;
+      reduce_all(v);
+      if (check && v[3] <= a.tol) conv = true;
+      if (!conv) alpha = bb_step(v, it);
+      if (recorder) {
+        if (check) sc->residual = v[3];
+        sc->alpha = alpha;
+        sc->converged = conv ? 1 : 0;
+        sc->iterations = it;
+      }
+      if (conv) break;
+      ++it;
+    }
+    if (recorder) sc->iterations = it;
+    if (!conv) return;
+    const long long tid = (long long)blockIdx.x * kBlock + threadIdx.x, stride = (long long)nb * kBlock;
+    for (long long c = tid; c < a.m; c += stride) a.phi[c] = ldcg(a.phin + c);
+    return;
+  }
 
   // gradient at gamma_0 and the initial residual (BBPGD.cpp:40-44)
   {
@@ -424,7 +483,6 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : Occupancy<Real>::kBlocksPerS
       sc->residual = v[3];
       sc->alpha = 1.0 / v[3];
       sc->converged = 0;
-      reset_take(sc);
     }
     if (TR)
       trace_record(smt, a.tr_part, nb, a.nchunks, a.dt, a.lambda, a.tau, 0, v[3], 1.0 / v[3], a.trace_out,
@@ -460,7 +518,6 @@ __global__ void __launch_bounds__(kBlock, kTr ? 1 : Occupancy<Real>::kBlocksPerS
         if (!conv) sc->alpha = bb_step(v, it);
         sc->converged = conv;
         sc->iterations = it;
-        reset_take(sc);
       }
     };
     if (!bar.sync_reduce(reduce_iter)) return;

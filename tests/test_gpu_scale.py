@@ -97,6 +97,18 @@ def matched_distance(a: dict, b: dict) -> float:
     return float(matched_distances(a, b).max())
 
 
+def within_reference_spread(what: str, got: float, ref: float, others: np.ndarray) -> tuple[float, float]:
+    """The reference's run (`ref`) and its runs with other division draws
+    (`others`) as one sample: `got` must lie within 3 standard deviations of
+    its mean.  Returns (mean, std)."""
+    runs = np.concatenate([[float(ref)], np.asarray(others, float)])
+    mean, std = float(runs.mean()), float(runs.std(ddof=1))
+    print(f"{what}: {got} against the reference's {ref} and {sorted(np.asarray(others).tolist())} "
+          f"(mean {mean:.1f}, std {std:.1f}, {abs(got - mean) / std:.2f} std from the mean)")
+    assert abs(got - mean) <= 3.0 * std, (what, got, mean, std)
+    return mean, std
+
+
 def check_contacts(fx: dict, prefix: str, tag: str, tol: float):
     p = params_of(fx)
     g = Colony(p)
@@ -178,6 +190,35 @@ def test_grown_colony_tight_solve_matches_reference():
                                        pos_factor=10.0)
 
 
+@pytest.mark.parametrize("name,prefix", [("dense_r40_seed0", ""), ("grown_hard_r20_seed0", "end_")])
+def test_multi_block_planar_solver_bit_identical_to_general(name, prefix):
+    """Above 1,024 cells the planar solve runs the multi-block kernel, whose
+    warps draw cell units from counters and whose blocks each reduce the
+    chunk partials themselves; the general 3D kernel runs the same chunks and
+    per-cell sums with a static cell order and one reducing block.  Two planar
+    solves and the general one give the same bits."""
+    fx = load_fixture(name)
+    cells = sub(fx, f"{prefix}cells_")
+    dt = float(fx[f"{prefix}dt"]) if f"{prefix}dt" in fx else float(params_of(fx).dt)
+    out = []
+    for variant in (abi.SOLVER_AUTO, abi.SOLVER_AUTO, abi.SOLVER_GENERAL):
+        g = Colony(params_of(fx, solver_variant=variant))
+        g.set_cells(cells)
+        g.profiling(True)
+        st = g.solve(dt, 0)
+        prof = g.profile()
+        assert prof["bbpgd_grid_launches"] >= 1 and prof["bbpgd_cta_launches"] == 0, prof
+        out.append((st, g.get_cells(), g.constraints()))
+    assert len(cells["x"]) > 1024
+    print(f"\n{name}: {out[0][0]['bbpgd_iterations']} iterations, {out[0][0]['relcp_iterations']} phases")
+    for other in out[1:]:
+        assert other[0] == out[0][0]
+        for k in ("x", "y", "z", "q0", "q3", "length", "ldot", "stress", "impedance", "force", "velocity"):
+            np.testing.assert_array_equal(other[1][k], out[0][1][k], err_msg=k)
+        for k in ("gamma", "sd"):
+            np.testing.assert_array_equal(other[2][k], out[0][2][k], err_msg=k)
+
+
 @pytest.mark.parametrize("snap", ["mid_", "end_"])
 def test_grown_colony_continuation_matches_reference(snap):
     """Ten full steps (divide, x-sort, ReLCP, move, grow) from each snapshot."""
@@ -214,9 +255,9 @@ def test_grown_colony_from_one_cell():
     matter, after which rounding differences in the solver make the
     trajectories part (division waves shift by a step or two); once the
     colony has 200 cells the counts must stay within 10 % of the reference's
-    at every step, and the run must reach
-    R = 20 within 1 % of the reference's step count with a final cell count
-    within 2 %."""
+    at every step, and the step count to R = 20 and the cell count there
+    must lie within 3 standard deviations of the reference's own runs (this
+    one and six with other division draws)."""
     fx = load_fixture("grown_hard_r20_seed0")
     p = params_of(fx)
     g = Colony(p)
@@ -236,8 +277,10 @@ def test_grown_colony_from_one_cell():
     print(f"\nsteps {len(got)} (reference {len(want)}), cells {got[-1]} (reference {want[-1]}), "
           f"identical cell counts through step {first_diff}, largest relative difference {rel.max():.3g}")
     assert radius >= 20.0
-    assert abs(len(got) - len(want)) <= 0.01 * len(want)
-    assert abs(int(got[-1]) - int(want[-1])) <= 0.02 * int(want[-1])
+    spread = load_fixture("spread_r20")
+    within_reference_spread("steps to R = 20", len(got), len(want), spread["hard_steps"])
+    within_reference_spread("cells at R = 20", int(got[-1]), int(want[-1]), spread["hard_final_cells"])
+    # identical growth until contacts matter (the division draws are the same)
     assert first_diff >= 2000
     big = want[:k] >= 200
     assert rel[big].max() <= 0.10
@@ -320,8 +363,9 @@ def test_adaptive_dt_trajectory_matches_reference():
 
 def test_soft_colony_grown_to_r20():
     """Config 1 end to end: the soft model from one cell to R = 20 at
-    dt = 3e-5 on the device, against the reference's run; then one force
-    assembly on the reference's final state."""
+    dt = 3e-5 on the device, against the spread of the reference's runs
+    (steps and cells at R = 20); then one force assembly on the reference's
+    final state."""
     fx = load_fixture("grown_soft_r20_seed0")
     p = params_of(fx)
     want = fx["hist_n_cells"]
@@ -330,8 +374,9 @@ def test_soft_colony_grown_to_r20():
     steps, cs, st = g.run(20.0, int(len(want) * 1.05))
     print(f"\nsoft: {steps} steps (reference {len(want)}), {st['n_cells']} cells (reference {want[-1]})")
     assert st["colony_radius"] >= 20.0
-    assert abs(steps - len(want)) <= 0.02 * len(want)
-    assert abs(st["n_cells"] - int(want[-1])) <= 0.02 * int(want[-1])
+    spread = load_fixture("spread_r20")
+    within_reference_spread("soft steps to R = 20", steps, len(want), spread["soft_steps"])
+    within_reference_spread("soft cells at R = 20", int(st["n_cells"]), int(want[-1]), spread["soft_final_cells"])
     g = Colony(p)
     g.set_cells(sub(fx, "end_cells_"))
     g.solve(p.dt, 0)
