@@ -342,7 +342,7 @@ def roofline(prof: dict, precision: str, peaks: dict) -> dict:
     bb_ms = prof["bbpgd_ms"]
     achieved = prof["bbpgd_algo_bytes"] / (bb_ms / 1e3) / 1e9 if bb_ms > 0 else 0.0
     mixed = precision == "mixed"
-    ratio = traffic_ratio("k_bbpgd_planar_mixed_frozen_r260" if mixed else "k_bbpgd_planar_frozen_r260")
+    ratio = traffic_ratio("k_bbpgd_planar_mixed_frozen_grown_r260" if mixed else "k_bbpgd_planar_frozen_grown_r260")
     launches_bb = max(prof["bbpgd_launches"], 1)
     return {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,

@@ -99,14 +99,18 @@ def matched_distance(a: dict, b: dict) -> float:
 
 def within_reference_spread(what: str, got: float, ref: float, others: np.ndarray) -> tuple[float, float]:
     """The reference's run (`ref`) and its runs with other division draws
-    (`others`) as one sample: `got` must lie within 3 standard deviations of
-    its mean.  Returns (mean, std)."""
+    (`others`) as one sample of n runs: `got` must lie in the 99 % prediction
+    interval of one more run, mean +- t(0.995, n - 1) s sqrt(1 + 1/n) (s the
+    sample standard deviation).  Returns (mean, half width)."""
+    from scipy.stats import t as student_t
     runs = np.concatenate([[float(ref)], np.asarray(others, float)])
-    mean, std = float(runs.mean()), float(runs.std(ddof=1))
+    n = runs.size
+    mean, sd = float(runs.mean()), float(runs.std(ddof=1))
+    half = float(student_t.ppf(0.995, n - 1)) * sd * np.sqrt(1.0 + 1.0 / n)
     print(f"{what}: {got} against the reference's {ref} and {sorted(np.asarray(others).tolist())} "
-          f"(mean {mean:.1f}, std {std:.1f}, {abs(got - mean) / std:.2f} std from the mean)")
-    assert abs(got - mean) <= 3.0 * std, (what, got, mean, std)
-    return mean, std
+          f"(mean {mean:.1f}, sd {sd:.1f}; 99 % prediction interval +-{half:.1f}, got {got - mean:+.1f})")
+    assert abs(got - mean) <= half, (what, got, mean, half)
+    return mean, half
 
 
 def check_contacts(fx: dict, prefix: str, tag: str, tol: float):
@@ -256,8 +260,8 @@ def test_grown_colony_from_one_cell():
     trajectories part (division waves shift by a step or two); once the
     colony has 200 cells the counts must stay within 10 % of the reference's
     at every step, and the step count to R = 20 and the cell count there
-    must lie within 3 standard deviations of the reference's own runs (this
-    one and six with other division draws)."""
+    must lie in the 99 % prediction interval of the reference's own runs
+    (this one and six with other division draws)."""
     fx = load_fixture("grown_hard_r20_seed0")
     p = params_of(fx)
     g = Colony(p)
