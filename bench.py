@@ -1,10 +1,11 @@
 """Benchmark of the collision hot path: cell-steps/s of the hard model.
 
-Workload (default): config 2 -- one colony grown by this library's plain FP64
-path from a single cell to radius 260 (the reference's largest published
-run: R = 260, about 3e5 cells), stored as the start state
+Workload (default): config 2 -- one colony grown by this library from a
+single cell to radius 260 in config 2's mixed precision (the reference's
+largest published run: R = 260, about 3e5 cells), stored as the start state
 proliferatingcellcollectives-idp_b200/data/colony_r260_seed0.npz (made by
-`bench.py --grow --radius 260 --precision fp64 --save ...`).  A step is one
+`bench.py --grow --radius 260 --precision mixed --save ...`, in two pieces
+joined by --checkpoint / --resume).  A step is one
 full simulator step on it through the C ABI -- divide, x-sort renumbering,
 the ReLCP loop of contact detection and BBPGD solves, motion, growth and
 the CFL time-step adaptation (capped at 1e-3) -- in config 2's mixed
@@ -590,7 +591,11 @@ def run_frozen(args):
     else:
         cells, dt0 = make_colony(args.radius, seed=0), 3e-4
     prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
-    col = device.Colony(colony_params(dt=dt0, capacity_hint=int(len(cells["x"]) * 1.5), precision=prec))
+    # --frozen-tol loosens the BBPGD tolerance of the frozen solves only, which
+    # bounds a launch's iterations (for a profiler capture); the traffic of one
+    # iteration does not depend on it
+    col = device.Colony(colony_params(dt=dt0, capacity_hint=int(len(cells["x"]) * 1.5), precision=prec,
+                                      tolerance=args.frozen_tol))
     col.set_cells(cells)
     for _ in range(args.warmup):
         col.step()
@@ -602,6 +607,7 @@ def run_frozen(args):
     m = int(round((prof["bbpgd_algo_bytes"] / max(prof["bbpgd_iterations"], 1) - bn * n) / bc))
     algo = it * (bc * m + bn * n)
     print(json.dumps({"frozen_bbpgd": True, "precision": args.precision, "start": args.start, "radius": args.radius,
+                      "tolerance": args.frozen_tol,
                       "cells": n, "constraints": m, "iterations": it, "us_per_iteration": ms * 1e3 / max(it, 1),
                       "residual": res, "ms_per_solve": ms, "algo_bytes_per_solve": algo,
                       "algo_gbs": algo / (ms / 1e3) / 1e9,
@@ -817,7 +823,7 @@ def run_jobs(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--radius", type=float, default=RADIUS)
@@ -827,6 +833,7 @@ def main():
                     help="BBPGD operand precision (mixed: FP32 D/L/M/U, FP64 gamma, dots, residual)")
     ap.add_argument("--verbose", action="store_true", help="per-step solver statistics on stderr")
     ap.add_argument("--frozen", action="store_true", help="BBPGD microbench on a frozen constraint set")
+    ap.add_argument("--frozen-tol", type=float, default=1e-3, help="--frozen: BBPGD tolerance of the frozen solves")
     ap.add_argument("--start", choices=["packing", "grown"], default="packing",
                     help="--frozen: the synthetic dense packing of --radius, or the grown R=260 colony")
     ap.add_argument("--jobs", type=int, default=0, help="batch sweep of N colonies (continuous batching)")
