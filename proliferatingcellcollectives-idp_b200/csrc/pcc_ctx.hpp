@@ -129,8 +129,8 @@ struct pcc_ctx {
   pcc::DevBuf<pcc::SolverScalars> scal;
   pcc::DevBuf<double> fel;  // soft: Hertz force magnitude per contact
   // packed operands of the planar solver
-  pcc::DevBuf<int2> p_ij, p_pos;
-  pcc::DevBuf<double2> p_n, p_t, p_s, p_gg, p_ev;
+  pcc::DevBuf<int2> p_ij;
+  pcc::DevBuf<double2> p_n, p_t, p_s, p_gg;
   pcc::DevBuf<double> p_gold, p_phin;
   pcc::DevBuf<double4> p_inc, p_cell, p_u;
   // ... their FP32 forms (mixed precision)

@@ -11,26 +11,31 @@
 // separated by grid barriers:
 //   cell pass: kLanes lanes per cell walk the cell's incidence entries
 //     (ascending constraint order, lane l takes entries l, l + kLanes, ...),
-//     each entry a coalesced read of its D row, the constraint's gamma_old and
-//     the (gamma, g) pair of the previous iteration; gamma_k =
+//     each entry a coalesced read of its D row and the constraint's
+//     gamma_old, and a read of the (gamma, g) pair of the previous iteration
+//     from the constraint itself (entry 2c + side); gamma_k =
 //     max(gamma_{k-1} - alpha g_{k-1}, 0) is formed on the fly, the lanes'
 //     sums of F = D^T (gamma_k - gamma_old) and sigma = L^T gamma_k are combined
 //     by a fixed shuffle tree, and the first lane forms U = M F, the growth
 //     rate and its change;
 //   constraint pass: a few constraints per thread in fixed chunks
 //     (chunk_count, chunk_lo), phi_next = Phi + dt D U - dt L dldot, the new
-//     (gamma_k, g_k) written over the constraint's previous pair and pushed
-//     over its two incidence entries (so the next cell pass reads them in
-//     order instead of gathering), and the three Barzilai-Borwein dot
-//     products and the residual reduced per chunk by a fixed shuffle tree.
-// The (gamma, g) pairs are updated in place: the cell pass reads the entry
-// copies before the first barrier and the constraint pass rewrites them
-// after it, and each constraint's pair is read and rewritten by the same
-// thread.  On residual iterations (the only ones that can end the solve) the
+//     (gamma_k, g_k) written over the constraint's previous pair, and the
+//     three Barzilai-Borwein dot products and the residual reduced per chunk
+//     by a fixed shuffle tree.
+// The (gamma, g) pairs are updated in place: the cell pass reads them before
+// the first barrier and the constraint pass rewrites them after it, and each
+// constraint's pair is read and rewritten by the same thread.  Gathering the
+// pairs costs a 32-byte sector per scattered read; pushing copies to the two
+// incidence entries instead (sequential reads in the cell pass) cost the same
+// sector per scattered 16-byte write and measured 1.5-1.65x slower per
+// iteration once the constraint set is several times the L2.  On residual
+// iterations (the only ones that can end the solve) the
 // constraint pass also stores gamma_{k-1}, the iterate the reference returns,
 // and phi_next, so nothing has to be kept from the previous iteration.
-// The last block to reach the second barrier reduces the chunk partials in a
-// fixed order and publishes the step size and the convergence decision.  The
+// After the second barrier every block reduces the chunk partials in the same
+// fixed order (in the traced form the last block to arrive does, and
+// publishes the step size and the convergence decision).  The
 // work of a chunk and of a cell never depends on which block does it, so the
 // result does not depend on the grid size: the one-CTA form for small
 // colonies (four 256-thread units in one block, named barriers instead of
@@ -104,7 +109,6 @@ struct PArgs {
   // per constraint
   const int2* ij;
   const V2 *nn, *tt, *ss;  // (n_x, n_y), (t_iz, t_jz), (s_i, s_j)
-  const int2* pos;         // incidence entries of side i and side j
   double* phi;             // Phi on entry, phi_next of the returned iterate on exit
   double* gamma;           // gamma_0 on entry, gamma_{k-1} on exit
   double* phin;            // phi_next of the last residual iteration
@@ -113,7 +117,7 @@ struct PArgs {
   const int* inc_off;
   const V4* inc;           // (D_x, D_y, D_t, s) of that side
   const double* gold;      // gamma_old of the entry's constraint
-  double2* ev;             // the entry's constraint's (gamma, g), a copy of gg
+  const int* ent;          // the entry's constraint and side (2c + side)
   // per cell
   const V4* cell;          // (M_lin, M_rot, len, ldot_prev)
   V4* u;                   // (u_x, u_y, w_z, dldot)
@@ -154,13 +158,12 @@ __device__ __forceinline__ void cell_pass(const PArgs<Real>& a, int mode, double
   constexpr bool kF64 = sizeof(Real) == 8;
   const int lane = threadIdx.x & 31, gl = lane % kLanes;
   constexpr long long kCellsPerWarp = 32 / kLanes;
-  const double2* ev = a.ev;
   auto accumulate = [&](CellAcc<Real>& A, int k) {
     const V4 d = a.inc[k];
     const double go = a.gold[k];
     double gc = go;
     if (mode != 0) {
-      const double2 s = ldcg(ev + k);
+      const double2 s = ldcg(a.gg + (a.ent[k] >> 1));
       gc = project(s.x, s.y, alpha);
     }
     const double diff = sub(gc, go);
@@ -346,7 +349,6 @@ template <class Real, class U, int kTr>
 __device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, double alpha, bool check, double* sm,
                                                 double* smt) {
   double2* gg = a.gg;
-  double2* eout = a.ev;
   for (long long ch = U::unit(); ch < a.nchunks; ch += U::units()) {
     double v[4] = {0, 0, 0, 0};
     double lin = 0.0;
@@ -362,9 +364,6 @@ __device__ __forceinline__ void constraint_pass(const PArgs<Real>& a, int mode, 
         a.gamma[c] = s.x;
         a.phin[c] = g;
       }
-      const int2 ps = a.pos[c];
-      eout[ps.x] = r;
-      eout[ps.y] = r;
       if (mode != 0) {
         const double dgm = sub(gam, s.x), dg = sub(g, s.y);
         v[0] = add(v[0], mul(dgm, dgm));
@@ -610,12 +609,10 @@ __global__ void k_pack_planar_cons(ConsView cs, long long m, int2* __restrict__ 
   gg0[c] = make_double2(cs.gamma[c], 0.0);
 }
 
-// Per incidence entry: its side's D row, the constraint's gamma_old, and the
-// entry's position recorded in pos[c] (x: side i, y: side j).
+// Per incidence entry: its side's D row and the constraint's gamma_old.
 template <class Real>
 __global__ void k_pack_planar_inc(ConsView cs, const int* __restrict__ inc_ent, long long ne,
-                                  typename PT<Real>::V4* __restrict__ inc, double* __restrict__ gold,
-                                  int* __restrict__ pos) {
+                                  typename PT<Real>::V4* __restrict__ inc, double* __restrict__ gold) {
   using V4 = typename PT<Real>::V4;
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ne) return;
@@ -627,7 +624,6 @@ __global__ void k_pack_planar_inc(ConsView cs, const int* __restrict__ inc_ent, 
   else
     inc[k] = mk4<V4>(-cs.nx[c], -cs.ny[c], cs.tjz[c], cs.sj[c]);
   gold[k] = cs.gamma[c];
-  pos[2 * c + side] = (int)k;
 }
 
 template <class Real>
@@ -668,9 +664,8 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   const size_t n = ctx->n, m = ctx->ncons, ne = 2 * m;
   const size_t mm = m + 1, nn = n + 1;
   cudaError_t e;
-  if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_pos.reserve(mm, 0, s)) || (e = ctx->p_gg.reserve(mm, 0, s)) ||
-      (e = ctx->p_phin.reserve(mm, 0, s)) || (e = ctx->p_gold.reserve(ne + 1, 0, s)) ||
-      (e = ctx->p_ev.reserve(ne + 1, 0, s)))
+  if ((e = ctx->p_ij.reserve(mm, 0, s)) || (e = ctx->p_gg.reserve(mm, 0, s)) || (e = ctx->p_phin.reserve(mm, 0, s)) ||
+      (e = ctx->p_gold.reserve(ne + 1, 0, s)))
     return e;
   if ((e = B::nn(ctx).reserve(mm, 0, s)) || (e = B::tt(ctx).reserve(mm, 0, s)) || (e = B::ss(ctx).reserve(mm, 0, s)) ||
       (e = B::inc(ctx).reserve(ne + 1, 0, s)) || (e = B::cell(ctx).reserve(nn, 0, s)) ||
@@ -683,8 +678,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
     k_pack_planar_cons<Real><<<grid_for((long long)m), kBlock, 0, s>>>(cv, (long long)m, ctx->p_ij.p, B::nn(ctx).p,
                                                                        B::tt(ctx).p, B::ss(ctx).p, ctx->p_gg.p);
     k_pack_planar_inc<Real><<<grid_for((long long)ne), kBlock, 0, s>>>(cv, ctx->inc_ent.p, (long long)ne,
-                                                                       B::inc(ctx).p, ctx->p_gold.p,
-                                                                       reinterpret_cast<int*>(ctx->p_pos.p));
+                                                                       B::inc(ctx).p, ctx->p_gold.p);
     ctx->launches += 2;
   }
   if (n) {
@@ -699,7 +693,6 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   a.nn = B::nn(ctx).p;
   a.tt = B::tt(ctx).p;
   a.ss = B::ss(ctx).p;
-  a.pos = ctx->p_pos.p;
   a.phi = cv.sd;
   a.gamma = cv.gamma;
   a.phin = ctx->p_phin.p;
@@ -707,7 +700,6 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   a.inc_off = ctx->inc_off.p;
   a.inc = B::inc(ctx).p;
   a.gold = ctx->p_gold.p;
-  a.ev = ctx->p_ev.p;
   a.cell = B::cell(ctx).p;
   a.u = B::u(ctx).p;
   a.uext = ctx->uext_active ? ctx->uext.p : nullptr;
@@ -723,6 +715,7 @@ cudaError_t launch(pcc_ctx* ctx, double dt, const PlanarTrace& tr, int* kind) {
   a.max_it = ctx->params.max_bbpgd_iterations;
   a.partials = reinterpret_cast<double4*>(ctx->partials.p);
   a.nchunks = nchunks;
+  a.ent = ctx->inc_ent.p;
   a.sc = ctx->scal.p;
   a.st_err = ctx->status;
   a.trace = tr.trace;
